@@ -1,0 +1,208 @@
+/*
+ * blackhole_native.h -- C ABI of the B200 (sm_100a) GRRT hot-loop library
+ * (libbhnative.so).
+ *
+ * Every entry point takes plain pointers and sizes.  Array arguments are
+ * DEVICE pointers on the calling GPU unless a parameter name starts with h_;
+ * `stream` is a cudaStream_t (NULL = legacy default stream).  Calls are
+ * asynchronous on `stream` unless stated otherwise.  Every function returns a
+ * bhn_status; on failure bhn_last_error() holds a message (thread-local).
+ *
+ * The plugin micro-kernels replace the PyO3 functions of the reference's
+ * native core (native/core/src/lib.rs) that python/blackhole_sim/
+ * native_kernels.py binds; their float64 results reproduce the reference's
+ * bit for bit.  Reference paths are relative to the reference project root.
+ */
+#ifndef BLACKHOLE_NATIVE_H
+#define BLACKHOLE_NATIVE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BHN_ABI_VERSION 1
+
+typedef enum bhn_status {
+    BHN_OK = 0,
+    BHN_ERR_VALUE = 1,       /* bad argument; the message matches the reference's ValueError text */
+    BHN_ERR_CUDA = 2,        /* CUDA runtime error */
+    BHN_ERR_DEVICE = 3,      /* a kernel reported a failure through its status word */
+    BHN_ERR_UNSUPPORTED = 4  /* not an sm_100 device, or a disabled feature */
+} bhn_status;
+
+/* Invalid-sample policies of native_kernels.py:15 / :342-350. */
+enum { BHN_POLICY_NAN = 0, BHN_POLICY_INITIAL = 1, BHN_POLICY_ZERO = 2 };
+
+/* Ray termination status (kerr.py:25 plus the optical-depth cutoff of
+ * accelerated_renderer.py:123-125). */
+enum {
+    BHN_RAY_MAX_STEPS = 0,
+    BHN_RAY_CAPTURED = 1,
+    BHN_RAY_ESCAPED = 2,
+    BHN_RAY_INVALID = 3,
+    BHN_RAY_OPAQUE = 4
+};
+
+/* ---- library ------------------------------------------------------------ */
+
+/* Replaces core_version() (native/core/src/lib.rs:19-22). */
+const char *bhn_core_version(void);
+/* Message of the last failure on this host thread ("" if none). */
+const char *bhn_last_error(void);
+/* Device properties of the current device (detect_arch() of lib.rs:24-35 is
+ * answered by the host binding; this reports the GPU side). */
+int bhn_device_info(int32_t *sm_count, int32_t *cc_major, int32_t *cc_minor, int64_t *global_mem_bytes);
+
+/* FP32 FMA throughput probe used as the denominator of the FP32 roofline (no
+ * reference counterpart: a measurement aid).  Launches SMs * blocks_per_sm
+ * blocks of 256 threads doing iters * 128 FMAs each; *flops receives the FLOP
+ * count (2 per FMA).  scratch: >= SMs * blocks_per_sm * 256 floats (never
+ * written in practice). */
+int bhn_fp32_peak_probe(float *scratch, int32_t iters, int32_t blocks_per_sm, int64_t *flops, void *stream);
+
+/* ---- plugin micro-kernels (float64, bit-exact with the reference) -------- */
+
+/* Replaces stokes_rk2_brick (native/core/src/lib.rs:227-279).  coeffs: cells*11,
+ * initial: 4 (broadcast) or 4*cells values, out: 4*cells. */
+int bhn_stokes_rk2_brick(const double *coeffs, int64_t cells, double ds_cm, const double *initial,
+                         int64_t initial_len, double *out, void *stream);
+
+/* Replaces sample_brick_trilinear (native/core/src/lib.rs:281-306).  coeffs:
+ * nr*nt*np*11 in [r][theta][phi][11] order, points: n*3 (r, theta, phi),
+ * out: n*11 with NaN rows outside the nonperiodic r/theta domain. */
+int bhn_sample_brick_trilinear(const double *coeffs, const double *r_grid, int64_t nr, const double *theta_grid,
+                               int64_t nt, const double *phi_grid, int64_t np, const double *points,
+                               int64_t n_points, double *out, void *stream);
+
+/* Replaces sample_and_step_stokes (native/core/src/lib.rs:308-366) and, for a
+ * policy other than BHN_POLICY_NAN, also the Python-side policy overwrite of
+ * native_kernels.py:391-397.  out: n*4. */
+int bhn_sample_and_step_stokes(const double *coeffs, const double *r_grid, int64_t nr, const double *theta_grid,
+                               int64_t nt, const double *phi_grid, int64_t np, const double *points,
+                               int64_t n_points, double ds_cm, const double *initial, int64_t initial_len,
+                               int32_t invalid_policy, double *out, void *stream);
+
+/* Replaces sample_brick_valid_mask (native_kernels.py:189-210, Python-only in
+ * the reference): inclusive r/theta bounds, phi ignored.  mask: n bytes (0/1). */
+int bhn_sample_brick_valid_mask(const double *r_grid, int64_t nr, const double *theta_grid, int64_t nt,
+                                const double *points, int64_t n_points, uint8_t *mask, void *stream);
+
+/* Input checks of native/core/src/lib.rs:112-169 on device data: counts[0] +=
+ * number of non-finite values; counts[1] += number of i with values[i+1] <=
+ * values[i] when check_increasing != 0.  counts: 2 device uint32 (zeroed by
+ * the caller). */
+int bhn_check_values(const double *values, int64_t n, int32_t check_increasing, uint32_t *counts, void *stream);
+
+/* ---- coefficient bricks for the fused renderer ---------------------------- */
+
+/* Record layout: one cell = 12 values (the 11 COEFF_NAMES channels of
+ * python/blackhole_sim/coefficient_bricks.py:21-25 plus one pad), float32
+ * records are 3 float4 (48 B), float64 records 6 double2 (96 B). */
+#define BHN_RECORD_VALUES 12
+
+/* Bytes of the grid-table buffer for an nr x nt x np brick. */
+int64_t bhn_brick_tables_bytes(int32_t nr, int32_t nt, int32_t np);
+
+/* Builds the lookup tables (grids, reciprocal spacings, closed-form index
+ * parameters) from the three strictly increasing float64 grids. */
+int bhn_brick_build_tables(const double *r_grid, int32_t nr, const double *theta_grid, int32_t nt,
+                           const double *phi_grid, int32_t np, void *tables, void *stream);
+
+/* Repacks [cells][11] coefficients (coeff_bytes 4 = float32, 8 = float64) into
+ * records of record_bytes 4 (float32) or 8 (float64); nonfinite[0] += number
+ * of non-finite inputs (device uint32, zeroed by the caller). */
+int bhn_brick_pack(const void *coeffs, int32_t coeff_bytes, int64_t cells, void *records, int32_t record_bytes,
+                   uint32_t *nonfinite, void *stream);
+
+/* Cell location used by the fused renderer, exposed for bit-exact checks:
+ * index[4*i..] = (i_r0, i_theta0, i_phi0, valid), weights[3*i..] = (w_r, w_theta,
+ * w_phi) as float.  Indices equal numpy.searchsorted(side="right") - 1 with
+ * the clamps of native_kernels.py:137-161. */
+int bhn_brick_locate(const void *tables, int32_t nr, int32_t nt, int32_t np, const double *points, int64_t n_points,
+                     int32_t *index, float *weights, void *stream);
+
+/* ---- fused ray renderer ----------------------------------------------------- */
+
+/* One camera view (kerr.py:155-233 LocalCamera, accelerated_renderer.py:36-46).
+ * Angles in radians except fov_y_deg / roll_deg.  The step is
+ * h = clamp(h_scale * r, h_min, h_max).  The view renders the rectangle
+ * [x0, x0+crop_w) x [y0, y0+crop_h) of a width x height image; its pixels are
+ * written row-major at out + out_offset. */
+typedef struct bhn_view {
+    double spin_a;
+    double r_obs, theta_obs, phi_obs;
+    double fov_y_deg, roll_deg;
+    double h_scale, h_min, h_max;
+    double escape_radius;
+    double affine_to_length_cm;
+    double max_optical_depth;
+    int32_t width, height;
+    int32_t x0, y0, crop_w, crop_h;
+    int32_t max_steps;
+    int32_t pad0;
+    int64_t out_offset;
+} bhn_view;
+
+/* Launch shape, chosen by the autotuner. */
+typedef struct bhn_render_config {
+    int32_t block_threads;   /* 64..512, multiple of 32 */
+    int32_t blocks_per_sm;   /* persistent grid = SM count * blocks_per_sm */
+    int32_t tile_w, tile_h;  /* ray order: rays of one tile are consecutive in the queue */
+    int32_t refill_min;      /* a warp refills its dead lanes once this many (1..32) are dead */
+    int32_t precision;       /* 0 = FP32 fused kernel, 1 = FP64 (oracle-matched) kernel */
+} bhn_render_config;
+
+/* Launch totals accumulated on the device (all zeroed by each launch). */
+typedef struct bhn_render_stats {
+    unsigned long long ray_steps;      /* geodesic RK2 steps executed by live rays */
+    unsigned long long brick_steps;    /* steps whose midpoint sample was inside the brick */
+    unsigned long long rays;           /* rays traced */
+    unsigned long long status[5];      /* rays per BHN_RAY_* */
+    unsigned long long queue_fetches;  /* work-queue atomics issued */
+    float max_h_drift;                 /* max over rays of max |H - H0| */
+    uint32_t error_flags;              /* nonzero: a kernel detected an inconsistency */
+} bhn_render_stats;
+
+/* Optional per-ray outputs (any pointer may be NULL), indexed like the image. */
+typedef struct bhn_ray_outputs {
+    int32_t *steps;
+    uint8_t *status;
+    float *h_drift;
+} bhn_ray_outputs;
+
+/* Bytes of device scratch a render over n_views views needs (work-queue head,
+ * per-view tables, launch totals). */
+int64_t bhn_render_scratch_bytes(int32_t n_views);
+
+/* Uploads and derives the per-view tables into scratch (h_views is host memory,
+ * copied before return).  Call again when the views change. */
+int bhn_render_prepare(const bhn_view *h_views, int32_t n_views, void *scratch, int64_t scratch_bytes,
+                       void *stream);
+
+/* Runs the fused persistent kernel over all prepared views: camera ray (FP64)
+ * -> RK2 Kerr geodesic -> midpoint brick gather -> Stokes RK2 -> optical-depth
+ * cutoff, per accelerated_renderer.py:100-150 and kerr.py:337-384.  records is
+ * float32 (precision 0) or float64 (precision 1) records; out is float4
+ * (precision 0) or double4 (precision 1) Stokes (I, Q, U, V) per pixel; stats
+ * (device, may be NULL) receives the launch totals. */
+int bhn_render_launch(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np, int32_t n_views,
+                      const bhn_render_config *cfg, void *out, const bhn_ray_outputs *ray_out, void *scratch,
+                      int64_t scratch_bytes, bhn_render_stats *stats, void *stream);
+
+/* CUDA-graph form of bhn_render_launch: captures the queue reset and the
+ * persistent launch once; bhn_graph_launch replays it on `stream`. */
+typedef struct bhn_graph bhn_graph;
+int bhn_graph_create(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np, int32_t n_views,
+                     const bhn_render_config *cfg, void *out, const bhn_ray_outputs *ray_out, void *scratch,
+                     int64_t scratch_bytes, bhn_render_stats *stats, bhn_graph **graph);
+int bhn_graph_launch(bhn_graph *graph, void *stream);
+int bhn_graph_destroy(bhn_graph *graph);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLACKHOLE_NATIVE_H */

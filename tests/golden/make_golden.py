@@ -1,0 +1,297 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a container where the reference project is mounted (read-only):
+
+    python tests/golden/make_golden.py --reference /root/reference/python
+
+Every output value in the fixtures is computed by the reference's own Python
+functions (python/blackhole_sim/native_kernels.py, kerr.py,
+accelerated_renderer.py).  The ray-loop fixtures compose those functions the
+way the brick renderer does (accelerated_renderer.py:129-150), with the RK2
+midpoint step of native/cuda/kerr_stokes_kernel.cu:13 in place of rk4_step and
+the variable step h = clamp(0.02 r, 1e-3, 1).  Inputs are seeded and stored
+beside the outputs, so the tests never need the reference at run time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import math
+import sys
+import time
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+
+
+def _linear_coeff_fixture(nphi: int = 2):
+    """The reference test fixture (python/tests/test_native_sampler_parity.py:22-35)."""
+    r_grid = np.array([0.0, 1.0])
+    theta_grid = np.array([0.0, 1.0])
+    phi_grid = np.array([0.0, 1.0]) if nphi == 2 else np.linspace(0.0, 2.0 * math.pi, nphi, endpoint=False)
+    coeffs = np.empty((2, 2, nphi, 11))
+    for ir in range(2):
+        for it in range(2):
+            for ip in range(nphi):
+                coeffs[ir, it, ip] = 100.0 * ir + 10.0 * it + ip + np.arange(11) * 0.125
+    return coeffs, r_grid, theta_grid, phi_grid
+
+
+def micro_kernels(nk, bench) -> dict[str, np.ndarray]:
+    out: dict[str, np.ndarray] = {}
+    rng = np.random.default_rng(20260101)
+
+    # (1) the reference test fixture with nphi=4 and edge points
+    c4, rg, tg, pg = _linear_coeff_fixture(4)
+    pts = np.array([
+        [0.25, 0.50, math.pi / 4.0],
+        [0.50, 0.25, 2.0 * math.pi + math.pi / 4.0],
+        [-0.10, 0.50, math.pi / 4.0],
+        [0.50, 1.10, math.pi / 4.0],
+        [1.00, 1.00, 0.0],                 # last knot in r and theta
+        [0.00, 0.00, -1.0e-3],             # first knot, negative phi
+        [0.50, 0.50, 3.0 * math.pi / 2.0], # exactly on a phi knot
+        [0.50, 0.50, 1.99 * math.pi],      # inside the wrap segment
+        [0.50, 0.50, -40.0 * math.pi + 0.3],
+        [1.0 + 1e-15, 0.5, 0.5],
+    ])
+    out["fix4_coeffs"], out["fix4_r"], out["fix4_theta"], out["fix4_phi"], out["fix4_points"] = c4, rg, tg, pg, pts
+    out["fix4_sample"] = nk.sample_brick_trilinear_reference(c4, rg, tg, pg, pts)
+    out["fix4_mask"] = nk.sample_brick_valid_mask(rg, tg, pts)
+    ini = np.zeros((pts.shape[0], 4))
+    ini[:, 0], ini[:, 1] = 1.0e-2, 1.0e-3
+    out["fix4_initial"] = ini
+    for pol in ("nan", "initial", "zero"):
+        out[f"fix4_step_{pol}"] = nk.sample_and_step_stokes_reference(c4, rg, tg, pg, pts, ds_cm=0.05, initial=ini,
+                                                                       invalid_policy=pol)
+
+    # (2) the reference benchmark fixture (benchmark.py:88-104), 8x6x8 brick, 64 points
+    coeffs, rg, tg, pg, pts = bench._sampler_fixture(8, 6, 8, 64)
+    out["bench_coeffs"], out["bench_r"], out["bench_theta"], out["bench_phi"], out["bench_points"] = coeffs, rg, tg, pg, pts
+    out["bench_sample"] = nk.sample_brick_trilinear_reference(coeffs, rg, tg, pg, pts)
+    for pol in ("nan", "initial", "zero"):
+        out[f"bench_step_{pol}"] = nk.sample_and_step_stokes_reference(coeffs, rg, tg, pg, pts, ds_cm=0.05,
+                                                                        initial=np.array([1e-2, 1e-3, 0.0, 0.0]),
+                                                                        invalid_policy=pol)
+
+    # (3) random irregular grids with points on knots, outside, and wrapped phi
+    nr, nt, nph = 7, 5, 6
+    rgr = np.cumsum(rng.uniform(0.1, 1.0, nr)) + 1.0
+    tgr = np.cumsum(rng.uniform(0.05, 0.5, nt))
+    pgr = np.sort(rng.uniform(0.0, 2.0 * math.pi, nph))
+    cr = rng.normal(size=(nr, nt, nph, 11))
+    n = 400
+    pr = np.empty((n, 3))
+    pr[:, 0] = rng.uniform(rgr[0] - 0.3, rgr[-1] + 0.3, n)
+    pr[:, 1] = rng.uniform(tgr[0] - 0.1, tgr[-1] + 0.1, n)
+    pr[:, 2] = rng.uniform(-30.0, 30.0, n)
+    knots = rng.integers(0, n, 120)
+    pr[knots[:40], 0] = rgr[rng.integers(0, nr, 40)]
+    pr[knots[40:80], 1] = tgr[rng.integers(0, nt, 40)]
+    pr[knots[80:], 2] = pgr[rng.integers(0, nph, 40)] + 2.0 * math.pi * rng.integers(-3, 4, 40)
+    out["rand_coeffs"], out["rand_r"], out["rand_theta"], out["rand_phi"], out["rand_points"] = cr, rgr, tgr, pgr, pr
+    out["rand_sample"] = nk.sample_brick_trilinear_reference(cr, rgr, tgr, pgr, pr)
+    out["rand_mask"] = nk.sample_brick_valid_mask(rgr, tgr, pr)
+    rini = rng.normal(size=(n, 4))
+    out["rand_initial"] = rini
+    for pol in ("nan", "initial", "zero"):
+        out[f"rand_step_{pol}"] = nk.sample_and_step_stokes_reference(cr, rgr, tgr, pgr, pr, ds_cm=0.37,
+                                                                       initial=rini, invalid_policy=pol)
+
+    # (4) Stokes RK2 over a brick (python/tests/test_native_stokes_parity.py:32-41)
+    dc = nk.deterministic_stokes_coefficients(4, 3, 5)
+    dini = np.zeros(dc.shape[:-1] + (4,))
+    dini[..., 0], dini[..., 1] = 1.0e-2, 1.0e-3
+    out["det_coeffs"], out["det_initial"] = dc, dini
+    out["det_step"] = nk.stokes_rk2_brick_reference(dc, ds_cm=0.05, initial=dini)
+    out["det_step_broadcast"] = nk.stokes_rk2_brick_reference(dc, ds_cm=0.3, initial=np.array([0.5, -0.1, 0.2, 0.05]))
+    out["rand_rk2_coeffs"] = rng.normal(size=(257, 11))
+    out["rand_rk2_initial"] = rng.normal(size=(257, 4))
+    out["rand_rk2_step"] = nk.stokes_rk2_brick_reference(out["rand_rk2_coeffs"], ds_cm=0.11,
+                                                         initial=out["rand_rk2_initial"])
+    return out
+
+
+def kerr_fixtures(kerr) -> dict[str, np.ndarray]:
+    out: dict[str, np.ndarray] = {}
+    rng = np.random.default_rng(99)
+    # camera rays: (r, incl_deg, fov, a, ndc_x, ndc_y, aspect, roll)
+    cams = [
+        (1000.0, 17.0, 2.0 * math.degrees(math.atan(20.0 / 1000.0)), 0.9375, 0.3, -0.7, 16.0 / 9.0, 0.0),
+        (1000.0, 60.0, 2.0 * math.degrees(math.atan(20.0 / 1000.0)), 0.998, -0.9, 0.9, 1.0, 0.0),
+        (55.0, 65.0, 32.0, 0.55, 0.1, 0.2, 16.0 / 9.0, 0.0),
+        (40.0, 62.0, 30.0, 0.6, 0.1, -0.2, 16.0 / 9.0, 12.0),
+        (500.0, 89.0, 5.0, 0.0, -0.01, 0.02, 1.5, 0.0),
+    ]
+    y0s, pts_, pps = [], [], []
+    for r, inc, fov, a, nx, ny, asp, roll in cams:
+        cam = kerr.LocalCamera.from_degrees(r=r, inclination_degrees=inc, fov_y_degrees=fov, roll_degrees=roll)
+        y0, pt, pp = kerr.camera_ray_initial_state(cam, a, nx, ny, asp)
+        y0s.append(y0), pts_.append(pt), pps.append(pp)
+    out["cam_params"] = np.array(cams)
+    out["cam_y0"], out["cam_pt"], out["cam_pphi"] = np.array(y0s), np.array(pts_), np.array(pps)
+
+    # RHS, Hamiltonian and metric at random states
+    n = 64
+    st = np.empty((n, 6))
+    st[:, 0] = 0.0
+    st[:, 1] = rng.uniform(1.5, 900.0, n)
+    st[:, 2] = rng.uniform(1e-3, math.pi - 1e-3, n)
+    st[:, 3] = rng.uniform(-10, 10, n)
+    st[:, 4] = rng.normal(size=n)
+    st[:, 5] = rng.normal(size=n) * 5
+    st[:4, 2] = [0.0, 1e-9, math.pi, math.pi - 1e-9]   # pole clamps
+    aa = rng.uniform(0.0, 0.998, n)
+    pt = -rng.uniform(0.5, 1.5, n)
+    pp = rng.normal(size=n) * 3
+    out["rhs_states"], out["rhs_a"], out["rhs_pt"], out["rhs_pphi"] = st, aa, pt, pp
+    out["rhs_out"] = np.array([kerr.kerr_geodesic_rhs(st[i], aa[i], pt[i], pp[i]) for i in range(n)])
+    out["ham_out"] = np.array([kerr.hamiltonian_null(st[i], aa[i], pt[i], pp[i]) for i in range(n)])
+    out["gcon_out"] = np.array([kerr.kerr_metric_contravariant(st[i, 1], st[i, 2], aa[i]) for i in range(n)])
+    out["gcov_out"] = np.array([kerr.kerr_metric_covariant(st[i, 1], st[i, 2], aa[i]) for i in range(n)])
+    h = rng.uniform(1e-3, 1.0, n)
+    out["rk2_h"] = h
+    out["rk2_out"] = np.array([rk2_step(kerr, st[i], h[i], aa[i], pt[i], pp[i]) for i in range(n)])
+    return out
+
+
+def rk2_step(kerr, y, h, a, p_t, p_phi):
+    """RK2 midpoint (native/cuda/kerr_stokes_kernel.cu:13) on kerr.kerr_geodesic_rhs,
+    theta clamped like kerr.rk4_step (kerr.py:312)."""
+    k1 = kerr.kerr_geodesic_rhs(y, a, p_t, p_phi)
+    mid = y + 0.5 * h * k1
+    k2 = kerr.kerr_geodesic_rhs(mid, a, p_t, p_phi)
+    out = y + h * k2
+    out[2] = kerr._safe_theta(float(out[2]))
+    return out
+
+
+def trace_rk2(kerr, y0, p_t, p_phi, a, h_scale, h_min, h_max, max_steps, escape_radius):
+    """kerr.trace_kerr_null_geodesic (kerr.py:337-384) with the RK2 step and
+    h = clamp(h_scale * r, h_min, h_max) evaluated at the start of each step."""
+    y = np.asarray(y0, dtype=float).copy()
+    r_plus = kerr.horizon_radius(a)
+    states = [y.copy()]
+    H0 = abs(kerr.hamiltonian_null(y, a, p_t, p_phi))
+    max_h_err = 0.0
+    status = "max_steps"
+    prev_r = float(y[1])
+    steps = 0
+    for i in range(1, max_steps + 1):
+        h = min(max(h_scale * float(y[1]), h_min), h_max)
+        try:
+            y = rk2_step(kerr, y, h, a, p_t, p_phi)
+            steps += 1
+            H = abs(kerr.hamiltonian_null(y, a, p_t, p_phi))
+        except (FloatingPointError, ValueError, OverflowError):
+            status = "invalid"
+            break
+        if not np.all(np.isfinite(y)):
+            status = "invalid"
+            break
+        max_h_err = max(max_h_err, abs(H - H0))
+        states.append(y.copy())
+        r = float(y[1])
+        if r <= r_plus * (1.0 + 2.0e-4):
+            status = "captured"
+            break
+        if r > escape_radius and r > prev_r:
+            status = "escaped"
+            break
+        prev_r = r
+    if len(states) == 0 or not np.allclose(states[-1], y):
+        states.append(y.copy())
+    return np.vstack(states), status, max_h_err, steps
+
+
+STATUS_CODES = {"max_steps": 0, "captured": 1, "escaped": 2, "invalid": 3}
+
+
+def render_reference(kerr, acc, view: dict, brick) -> dict[str, np.ndarray]:
+    """Per-pixel composition of accelerated_renderer.render_tile_stokes_bricks
+    (accelerated_renderer.py:129-150) over the crop rectangle."""
+    W, H = view["width"], view["height"]
+    cam = kerr.LocalCamera.from_degrees(r=view["r_obs"], inclination_degrees=view["inclination_deg"],
+                                        phi_degrees=0.0, fov_y_degrees=view["fov_y_deg"])
+    aspect = W / H
+    x0, y0, cw, ch = view["crop"]
+    img = np.zeros((ch, cw, 4))
+    steps = np.zeros((ch, cw), dtype=np.int32)
+    status = np.zeros((ch, cw), dtype=np.int32)
+    drift = np.zeros((ch, cw))
+    bricks = SimpleNamespace(r=brick.r, theta=brick.theta, phi=brick.phi, coeffs=brick.coeffs.astype(np.float64))
+    for tj in range(ch):
+        j = y0 + tj
+        ndc_y = 1.0 - 2.0 * (j + 0.5) / H
+        for ti in range(cw):
+            i = x0 + ti
+            ndc_x = 2.0 * (i + 0.5) / W - 1.0
+            yy, pt, pp = kerr.camera_ray_initial_state(cam, view["spin_a"], ndc_x, ndc_y, aspect)
+            states, st, herr, n = trace_rk2(kerr, yy, pt, pp, view["spin_a"], view["h_scale"], view["h_min"],
+                                            view["h_max"], view["max_steps"], view["escape_radius"])
+            img[tj, ti] = acc.integrate_stokes_from_bricks_trace(states, bricks, affine_to_length_cm=1.0,
+                                                                 max_optical_depth=30.0)
+            steps[tj, ti], status[tj, ti], drift[tj, ti] = n, STATUS_CODES[st], herr
+    return {"stokes": img, "steps": steps, "status": status, "h_drift": drift}
+
+
+RAY_VIEWS = {
+    # the CPU-runnable configuration as stated: 32x18, r_obs 1000, 64 steps -> all-zero image
+    "c1": dict(width=32, height=18, r_obs=1000.0, inclination_deg=17.0,
+               fov_y_deg=2.0 * math.degrees(math.atan(20.0 / 1000.0)), spin_a=0.9375, max_steps=64,
+               h_scale=0.02, h_min=1e-3, h_max=1.0, escape_radius=220.0, crop=(0, 0, 32, 18)),
+    # nonzero variant: same geometry, enough steps to reach and cross the brick (central 12x8 crop)
+    "c1_long": dict(width=32, height=18, r_obs=1000.0, inclination_deg=17.0,
+                    fov_y_deg=2.0 * math.degrees(math.atan(20.0 / 1000.0)), spin_a=0.9375, max_steps=1600,
+                    h_scale=0.02, h_min=1e-3, h_max=1.0, escape_radius=220.0, crop=(10, 5, 12, 8)),
+    # the reference renderer's default camera distance (accelerated_renderer.py:40): r_obs 55, 65 deg
+    "near": dict(width=16, height=12, r_obs=55.0, inclination_deg=65.0, fov_y_deg=32.0, spin_a=0.9375,
+                 max_steps=700, h_scale=0.02, h_min=1e-3, h_max=1.0, escape_radius=220.0, crop=(0, 0, 16, 12)),
+}
+
+
+def ray_fixtures(kerr, acc, bricks_mod) -> dict[str, np.ndarray]:
+    out: dict[str, np.ndarray] = {}
+    brick = bricks_mod.torus_brick(8, 6, 8, spin_a=0.9375, seed=7, dtype=np.float64)
+    out["brick_coeffs"], out["brick_r"], out["brick_theta"], out["brick_phi"] = (brick.coeffs, brick.r,
+                                                                                  brick.theta, brick.phi)
+    for name, view in RAY_VIEWS.items():
+        t0 = time.time()
+        res = render_reference(kerr, acc, view, brick)
+        for k, v in res.items():
+            out[f"{name}_{k}"] = v
+        out[f"{name}_view"] = np.array([view["width"], view["height"], view["r_obs"], view["inclination_deg"],
+                                        view["fov_y_deg"], view["spin_a"], view["max_steps"], view["h_scale"],
+                                        view["h_min"], view["h_max"], view["escape_radius"], *view["crop"]])
+        print(f"  {name}: {time.time() - t0:.1f}s  nonzero={np.count_nonzero(res['stokes'][..., 0])}", flush=True)
+    return out
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference/python")
+    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray")
+    args = ap.parse_args()
+    sys.path.insert(0, args.reference)
+    sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
+    from blackhole_sim import accelerated_renderer as acc, benchmark as bench, kerr, native_kernels as nk
+    from blackhole_native import bricks as bricks_mod
+
+    only = set(filter(None, args.only.split(",")))
+    if not only or "micro" in only:
+        np.savez_compressed(HERE / "micro_kernels.npz", **micro_kernels(nk, bench))
+        print("wrote micro_kernels.npz")
+    if not only or "kerr" in only:
+        np.savez_compressed(HERE / "kerr.npz", **kerr_fixtures(kerr))
+        print("wrote kerr.npz")
+    if not only or "ray" in only:
+        np.savez_compressed(HERE / "ray_loop.npz", **ray_fixtures(kerr, acc, bricks_mod))
+        print("wrote ray_loop.npz")
+
+
+if __name__ == "__main__":
+    main()
