@@ -214,10 +214,14 @@ def run_oracle(brick, n: int, threads: int = 0) -> tuple[int, float]:
 
 
 def calibrated_oracle_size(brick, target_s: float) -> int:
-    """Side n of the n x n oracle sample that takes about target_s seconds."""
-    steps, dt = run_oracle(brick, 32)
-    n = int(32 * math.sqrt(max(target_s, 0.1) / max(dt, 1e-3)))
-    return max(32, min(1024, n))
+    """Side n of the n x n oracle sample that takes about target_s seconds
+    (two rounds: the first, tiny sample under-uses the threads)."""
+    n = 48
+    for _ in range(2):
+        steps, dt = run_oracle(brick, n)
+        n = int(n * math.sqrt(max(target_s, 0.1) / max(dt, 1e-3)) * (0.5 if n == 48 else 1.0))
+        n = max(32, min(1024, n))
+    return n
 
 
 def cpu_baseline(brick, target_s: float = 12.0) -> dict:
@@ -244,7 +248,10 @@ def bench_ours(args) -> dict | None:
 
     brick_h = make_brick()
     db = bn.DeviceBrick(brick_h, device=device, precisions=("fp32",))
-    view = bn.View(**WORKLOAD)
+    wl = dict(WORKLOAD)
+    if args.side:  # a smaller image of the same scene (profiling runs)
+        wl.update(width=args.side, height=args.side)
+    view = bn.View(**wl)
     cfg = bn.RenderConfig(**args.config) if args.config else None
     if cfg is None:
         from blackhole_native import autotune
@@ -357,9 +364,9 @@ def bench_ours(args) -> dict | None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "plain fused kernel at scale: 1024x1024 rays, r_obs=1000M, i=17deg, FOV +-20M, "
-                               "a=0.9375, RK2 h=0.02r in [1e-3,1], max_steps=4096, 256x128x256x11 float32 "
-                               "seeded torus brick",
+        "config": {"workload": f"plain fused kernel at scale: {view.width}x{view.height} rays, r_obs=1000M, "
+                               "i=17deg, FOV +-20M, a=0.9375, RK2 h=0.02r in [1e-3,1], max_steps=4096, "
+                               "256x128x256x11 float32 seeded torus brick",
                    "rays_per_step": rays, "ray_steps_per_step": steps_per_launch,
                    "brick_steps_per_step": brick_steps, "l2": "inputs larger than L2 (403 MB brick records)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -422,6 +429,8 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")
+    ap.add_argument("--side", type=int, default=0,
+                    help="render side x side rays of the same scene instead of 1024x1024 (profiling only)")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, whatever is asked
     line = bench_reference(args) if args.impl == "reference" else bench_ours(args)

@@ -79,6 +79,8 @@ class RenderStatsStruct(ctypes.Structure):
         ("queue_fetches", ctypes.c_ulonglong),
         ("max_h_drift", ctypes.c_float),
         ("error_flags", ctypes.c_uint32),
+        ("max_h_drift_escaped", ctypes.c_float),
+        ("pad0", ctypes.c_uint32),
     ]
 
 

@@ -215,6 +215,7 @@ class RenderStats:
     queue_fetches: int
     max_h_drift: float
     error_flags: int
+    max_h_drift_escaped: float
 
     @classmethod
     def from_device(cls, t: torch.Tensor) -> "RenderStats":
@@ -222,7 +223,7 @@ class RenderStats:
         s = _lib.RenderStatsStruct.from_buffer_copy(raw)
         return cls(int(s.ray_steps), int(s.brick_steps), int(s.rays),
                    {name: int(s.status[i]) for i, name in enumerate(_lib.RAY_STATUS)}, int(s.queue_fetches),
-                   float(s.max_h_drift), int(s.error_flags))
+                   float(s.max_h_drift), int(s.error_flags), float(s.max_h_drift_escaped))
 
 
 @dataclass

@@ -144,7 +144,7 @@ struct __align__(16) ViewDev {
     double e_r, e_th, e_ph;            // ZAMO tetrad scalings (kerr.py:144-148)
     double gcov00, gcov03, gcov11, gcov22, gcov33;
     double gcon00, gcon03, gcon11, gcon22, gcon33;
-    double r_capture, escape_radius;
+    double r_capture, escape_radius, r_plus, r_minus;
     double h_scale, h_min, h_max, L, max_tau;
     double width_d, height_d;          // image size as doubles (divisors of accelerated_renderer.py:138-140)
     int32_t width, height, x0, y0, crop_w, crop_h, max_steps, has_roll;

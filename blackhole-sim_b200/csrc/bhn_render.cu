@@ -86,7 +86,9 @@ __global__ void setup_views_kernel(const bhn_view *__restrict__ raw, int n, View
         d.sin_roll = sin(v.roll_deg * deg);
         d.width_d = (double)v.width;
         d.height_d = (double)v.height;
-        d.r_capture = (1.0 + sqrt(1.0 - a * a)) * (1.0 + 2.0e-4);  // kerr.py:371
+        d.r_plus = 1.0 + sqrt(1.0 - a * a);   // kerr.py:39-42
+        d.r_minus = 1.0 - sqrt(1.0 - a * a);
+        d.r_capture = d.r_plus * (1.0 + 2.0e-4);  // kerr.py:371
         d.escape_radius = v.escape_radius;
         d.h_scale = v.h_scale;
         d.h_min = v.h_min;
@@ -180,7 +182,7 @@ __device__ __forceinline__ CameraRay camera_ray(const ViewDev &v, int px, int py
 struct LaneCounters {
     unsigned long long steps, brick;
     uint32_t rays, status[5];
-    float max_drift;
+    float max_drift, max_drift_escaped;
 };
 
 struct RenderParams {
@@ -247,10 +249,17 @@ struct Deriv32 {
 // which is g^{mu nu} p_mu p_nu of kerr.py:86-102 regrouped; x' = dH/dp and
 // p' = -dH/dx are its exact derivatives (the quotient-rule sums of
 // kerr.py:236-282 collapse to these few terms).
-__device__ __forceinline__ void rhs32(float r, float s, float c, float pr, float pth, float pt, float pphi, float a,
-                                      float a2, Deriv32 &d) {
+//
+// Delta is evaluated as (r - r+)(r - r-) from the FP64 horizon distance
+// r - r+: the expanded r^2 - 2r + a^2 cancels to nothing in FP32 within ~1e-7
+// of the horizon, where 1/Delta then overflows (the horizon-proximity FP64
+// island).
+__device__ __forceinline__ void rhs32(double rd, double r_plus, float dpm, float s, float c, float pr, float pth,
+                                      float pt, float pphi, float a, float a2, Deriv32 &d) {
+    const float r = (float)rd;
+    const float x = (float)(rd - r_plus);
     const float r2 = r * r;
-    const float D = fmaf(r, r - 2.0f, a2);
+    const float D = x * (x + dpm);
     const float Sg = fmaf(a2 * c, c, r2);
     const float iS = 1.0f / Sg;
     const float iD = 1.0f / D;
@@ -271,10 +280,10 @@ __device__ __forceinline__ void rhs32(float r, float s, float c, float pr, float
 
 struct Tracer32 {
     double r, th, ph;
-    float pr, pth, pt, pphi, a, a2;
+    float pr, pth, pt, pphi, a, a2, dpm;
     float S0, S1, S2, S3, tau, drift, H0;
     float hs, hmin, hmax, L, max_tau;
-    double r_cap, esc;
+    double r_cap, esc, r_plus;
     int steps, brick, max_steps;
     bool poison;
     int64_t out_idx;
@@ -290,6 +299,8 @@ struct Tracer32 {
         pphi = (float)c.pphi;
         a = (float)v.a;
         a2 = a * a;
+        r_plus = v.r_plus;
+        dpm = (float)(v.r_plus - v.r_minus);
         H0 = (float)c.H0;
         S0 = S1 = S2 = S3 = 0.0f;
         tau = 0.0f;
@@ -316,14 +327,14 @@ struct Tracer32 {
         float s, c;
         pole_sincos(th, s, c);
         Deriv32 k1;
-        rhs32(rf, s, c, pr, pth, pt, pphi, a, a2, k1);
+        rhs32(r, r_plus, dpm, s, c, pr, pth, pt, pphi, a, a2, k1);
         drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
         const float hh = 0.5f * h;
         const double rm = r + (double)(hh * k1.r);
         const double thm = safe_theta(th + (double)(hh * k1.th));
         pole_sincos(thm, s, c);
         Deriv32 k2;
-        rhs32((float)rm, s, c, fmaf(hh, k1.pr, pr), fmaf(hh, k1.pth, pth), pt, pphi, a, a2, k2);
+        rhs32(rm, r_plus, dpm, s, c, fmaf(hh, k1.pr, pr), fmaf(hh, k1.pth, pth), pt, pphi, a, a2, k2);
         const float dr = h * k2.r, dph = h * k2.ph;
         const double rn = r + (double)dr;
         const double thn = safe_theta(th + (double)(h * k2.th));
@@ -423,7 +434,7 @@ struct Tracer32 {
             float s, c;
             pole_sincos(th, s, c);
             Deriv32 k;
-            rhs32((float)r, s, c, pr, pth, pt, pphi, a, a2, k);
+            rhs32(r, r_plus, dpm, s, c, pr, pth, pt, pphi, a, a2, k);
             drift = fmaxf(drift, fabsf(fabsf(k.H) - H0));
         }
         float4 o;
@@ -693,6 +704,7 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
     cnt.rays = 0;
     for (int k = 0; k < 5; ++k) cnt.status[k] = 0;
     cnt.max_drift = 0.0f;
+    cnt.max_drift_escaped = 0.0f;
     unsigned long long fetches = 0;
 
     while (true) {
@@ -717,7 +729,9 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
                         // no step is taken: the reference returns a zero Stokes vector
                         Tracer::write_zero(P.out, px.out_idx);
                         cnt.rays += 1;
-                        cnt.status[v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID] += 1;
+                        const int zst = v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID;
+#pragma unroll
+                        for (int k = 0; k < 5; ++k) cnt.status[k] += (zst == k);
                         if (P.ray_steps) P.ray_steps[px.out_idx] = 0;
                         if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)(v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID);
                         if (P.ray_drift) P.ray_drift[px.out_idx] = 0.0f;
@@ -736,8 +750,10 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
                 cnt.steps += (unsigned long long)tr.steps;
                 cnt.brick += (unsigned long long)tr.brick;
                 cnt.rays += 1;
-                cnt.status[st] += 1;
+#pragma unroll
+                for (int k = 0; k < 5; ++k) cnt.status[k] += (st == k);
                 cnt.max_drift = fmaxf(cnt.max_drift, (float)tr.drift);
+                if (st == BHN_RAY_ESCAPED) cnt.max_drift_escaped = fmaxf(cnt.max_drift_escaped, (float)tr.drift);
                 if (P.ray_steps) P.ray_steps[tr.out_idx] = tr.steps;
                 if (P.ray_status) P.ray_status[tr.out_idx] = (uint8_t)st;
                 if (P.ray_drift) P.ray_drift[tr.out_idx] = (float)tr.drift;
@@ -751,8 +767,10 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
         cnt.steps += __shfl_down_sync(kFull, cnt.steps, o);
         cnt.brick += __shfl_down_sync(kFull, cnt.brick, o);
         cnt.rays += __shfl_down_sync(kFull, cnt.rays, o);
+#pragma unroll
         for (int k = 0; k < 5; ++k) cnt.status[k] += __shfl_down_sync(kFull, cnt.status[k], o);
         cnt.max_drift = fmaxf(cnt.max_drift, __shfl_down_sync(kFull, cnt.max_drift, o));
+        cnt.max_drift_escaped = fmaxf(cnt.max_drift_escaped, __shfl_down_sync(kFull, cnt.max_drift_escaped, o));
     }
     if (lane == 0 && P.stats) {
         atomicAdd(&P.stats->ray_steps, cnt.steps);
@@ -763,6 +781,8 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
         atomicAdd(&P.stats->queue_fetches, fetches);
         // non-negative floats order like their bit patterns
         atomicMax(reinterpret_cast<unsigned int *>(&P.stats->max_h_drift), __float_as_uint(cnt.max_drift));
+        atomicMax(reinterpret_cast<unsigned int *>(&P.stats->max_h_drift_escaped),
+                  __float_as_uint(cnt.max_drift_escaped));
     }
 }
 

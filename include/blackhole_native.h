@@ -162,8 +162,11 @@ typedef struct bhn_render_stats {
     unsigned long long rays;           /* rays traced */
     unsigned long long status[5];      /* rays per BHN_RAY_* */
     unsigned long long queue_fetches;  /* work-queue atomics issued */
-    float max_h_drift;                 /* max over rays of max |H - H0| */
+    float max_h_drift;                 /* max over rays of max |H - H0| (kerr.py:352, 367) */
     uint32_t error_flags;              /* nonzero: a kernel detected an inconsistency */
+    float max_h_drift_escaped;         /* the same over escaped rays only (a captured ray's last
+                                          state sits at the horizon, where H is ill-conditioned) */
+    uint32_t pad0;
 } bhn_render_stats;
 
 /* Optional per-ray outputs (any pointer may be NULL), indexed like the image. */
