@@ -252,6 +252,12 @@ def bench_ours(args) -> dict | None:
     if args.side:  # a smaller image of the same scene (profiling runs)
         wl.update(width=args.side, height=args.side)
     view = bn.View(**wl)
+    if args.tune:
+        from blackhole_native import autotune
+
+        best = autotune.tune(db, [view], "config2", log=lambda m: print(m, file=sys.stderr, flush=True))
+        print(json.dumps({"autotune": "config2", "best": best.__dict__, "cache": str(autotune.CACHE)}), flush=True)
+        return None
     cfg = bn.RenderConfig(**args.config) if args.config else None
     if cfg is None:
         from blackhole_native import autotune
@@ -429,6 +435,7 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")
+    ap.add_argument("--tune", action="store_true", help="run the launch-shape autotuner on the workload and exit")
     ap.add_argument("--side", type=int, default=0,
                     help="render side x side rays of the same scene instead of 1024x1024 (profiling only)")
     args = ap.parse_args(argv)

@@ -50,7 +50,7 @@ class ViewStruct(ctypes.Structure):
         ("crop_w", ctypes.c_int32),
         ("crop_h", ctypes.c_int32),
         ("max_steps", ctypes.c_int32),
-        ("pad0", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
         ("out_offset", ctypes.c_int64),
     ]
 
@@ -65,6 +65,7 @@ class RenderConfigStruct(ctypes.Structure):
         ("tile_h", ctypes.c_int32),
         ("refill_min", ctypes.c_int32),
         ("precision", ctypes.c_int32),
+        ("reg_cap", ctypes.c_int32),
     ]
 
 

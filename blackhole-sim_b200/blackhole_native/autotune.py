@@ -14,7 +14,7 @@ from __future__ import annotations
 import itertools
 import json
 import os
-from dataclasses import asdict
+from dataclasses import asdict, replace
 from pathlib import Path
 from typing import Callable, Iterable, Sequence
 
@@ -29,6 +29,7 @@ DEFAULT_SPACE = {
     "blocks_per_sm": (2, 4, 8),
     "tile": ((8, 4), (4, 8), (16, 2), (32, 1)),
     "refill_min": (1, 8, 16, 32),
+    "reg_cap": (0, 80, 64),
 }
 
 
@@ -57,13 +58,28 @@ def store(workload: str, config: RenderConfig, ms: float, device: torch.device, 
     CACHE.write_text(json.dumps(data, indent=1, sort_keys=True) + "\n")
 
 
-def candidates(space: dict | None = None) -> Iterable[RenderConfig]:
+def launch_candidates(space: dict | None = None, base: RenderConfig | None = None) -> Iterable[RenderConfig]:
+    """Stage 1: threads per block x resident blocks x register budget."""
     s = space or DEFAULT_SPACE
-    for bt, bps, (tw, th), rm in itertools.product(s["block_threads"], s["blocks_per_sm"], s["tile"],
-                                                  s["refill_min"]):
+    b = base or RenderConfig()
+    for bt, bps, rc in itertools.product(s["block_threads"], s["blocks_per_sm"], s["reg_cap"]):
         if bt * bps > 2048:   # more threads than an SM holds
             continue
-        yield RenderConfig(block_threads=bt, blocks_per_sm=bps, tile_w=tw, tile_h=th, refill_min=rm)
+        yield replace(b, block_threads=bt, blocks_per_sm=bps, reg_cap=rc)
+
+
+def order_candidates(space: dict | None = None, base: RenderConfig | None = None) -> Iterable[RenderConfig]:
+    """Stage 2: ray-order tile x warp refill threshold, on the best launch shape."""
+    s = space or DEFAULT_SPACE
+    b = base or RenderConfig()
+    for (tw, th), rm in itertools.product(s["tile"], s["refill_min"]):
+        yield replace(b, tile_w=tw, tile_h=th, refill_min=rm)
+
+
+def candidates(space: dict | None = None) -> Iterable[RenderConfig]:
+    """The full product of both stages (for exhaustive sweeps)."""
+    for c in launch_candidates(space):
+        yield from order_candidates(space, c)
 
 
 def time_config(brick: DeviceBrick, views: Sequence[View], cfg: RenderConfig, *, precision: str = "fp32",
@@ -89,15 +105,17 @@ def time_config(brick: DeviceBrick, views: Sequence[View], cfg: RenderConfig, *,
 
 def tune(brick: DeviceBrick, views: Sequence[View], workload: str, *, space: dict | None = None,
          precision: str = "fp32", repeats: int = 3, log: Callable[[str], None] | None = None) -> RenderConfig:
-    """Time every candidate, cache and return the fastest."""
+    """Two-stage search (launch shape, then ray order on the winner); caches and
+    returns the fastest configuration."""
     device = brick.device
-    best, best_ms, table = None, float("inf"), []
-    for cfg in candidates(space):
-        ms = time_config(brick, views, cfg, precision=precision, repeats=repeats)
-        table.append([asdict(cfg), round(ms, 4)])
-        if log:
-            log(f"{asdict(cfg)} {ms:.3f} ms")
-        if ms < best_ms:
-            best, best_ms = cfg, ms
+    best, best_ms, table = RenderConfig(), float("inf"), []
+    for stage in (launch_candidates, order_candidates):
+        for cfg in stage(space, best):
+            ms = time_config(brick, views, cfg, precision=precision, repeats=repeats)
+            table.append([asdict(cfg), round(ms, 4)])
+            if log:
+                log(f"{asdict(cfg)} {ms:.3f} ms")
+            if ms < best_ms:
+                best, best_ms = cfg, ms
     store(workload, best, best_ms, device, table)
     return best

@@ -54,6 +54,11 @@ class View:
     affine_to_length_cm: float = 1.0
     max_optical_depth: float = 30.0
     crop: tuple[int, int, int, int] | None = None  # (x0, y0, w, h) of the rendered rectangle
+    # Off: the reference's semantics.  On: an inbound ray inside both the innermost
+    # photon orbit and the brick's inner radius is captured at that step (no
+    # emission can follow in exact arithmetic), which stops the fixed h = 0.02 r
+    # step from overshooting into the horizon and flinging the ray back out.
+    horizon_guard: bool = False
 
     @property
     def rect(self) -> tuple[int, int, int, int]:
@@ -102,6 +107,7 @@ class View:
         s.width, s.height = int(self.width), int(self.height)
         s.x0, s.y0, s.crop_w, s.crop_h = int(x0), int(y0), int(w), int(h)
         s.max_steps = int(self.max_steps)
+        s.flags = 1 if self.horizon_guard else 0
         s.out_offset = int(out_offset)
         return s
 
@@ -115,12 +121,14 @@ class RenderConfig:
     tile_w: int = 8
     tile_h: int = 4
     refill_min: int = 1
+    reg_cap: int = 80
 
     def to_struct(self, precision: int) -> _lib.RenderConfigStruct:
         c = _lib.RenderConfigStruct()
         c.block_threads, c.blocks_per_sm = int(self.block_threads), int(self.blocks_per_sm)
         c.tile_w, c.tile_h, c.refill_min = int(self.tile_w), int(self.tile_h), int(self.refill_min)
         c.precision = int(precision)
+        c.reg_cap = int(self.reg_cap)
         return c
 
 

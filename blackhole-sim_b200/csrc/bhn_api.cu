@@ -216,6 +216,10 @@ __global__ void build_tables_kernel(const double *__restrict__ rg, int nr, const
     for (int i = threadIdx.x; i < nt; i += blockDim.x) idt[i] = i + 1 < nt ? (float)(1.0 / (tg[i + 1] - tg[i])) : 0.0f;
     for (int i = threadIdx.x; i < np; i += blockDim.x)
         idp[i] = (float)(1.0 / ((i + 1 < np ? pg[i + 1] : pg[0] + kTwoPi) - pg[i]));
+    float *grf = const_cast<float *>(T.grf), *gtf = const_cast<float *>(T.gtf), *gpf = const_cast<float *>(T.gpf);
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) grf[i] = (float)rg[i];
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) gtf[i] = (float)tg[i];
+    for (int i = threadIdx.x; i < np; i += blockDim.x) gpf[i] = (float)pg[i];
     if (threadIdx.x < 3) {
         const double *g = threadIdx.x == 0 ? rg : (threadIdx.x == 1 ? tg : pg);
         int n = threadIdx.x == 0 ? nr : (threadIdx.x == 1 ? nt : np);
@@ -239,9 +243,9 @@ __global__ void build_tables_kernel(const double *__restrict__ rg, int nr, const
                 off = log(g[0]) * inv;
             }
         }
-        if (threadIdx.x == 0) { h->kind_r = kind; h->off_r = off; h->inv_r = inv; }
-        if (threadIdx.x == 1) { h->kind_t = kind; h->off_t = off; h->inv_t = inv; }
-        if (threadIdx.x == 2) { h->kind_p = kind; h->off_p = off; h->inv_p = inv; }
+        if (threadIdx.x == 0) { h->kind_r = kind; h->off_r = off; h->inv_r = inv; h->foff_r = (float)off; h->finv_r = (float)inv; }
+        if (threadIdx.x == 1) { h->kind_t = kind; h->off_t = off; h->inv_t = inv; h->foff_t = (float)off; h->finv_t = (float)inv; }
+        if (threadIdx.x == 2) { h->kind_p = kind; h->off_p = off; h->inv_p = inv; h->foff_p = (float)off; h->finv_p = (float)inv; }
     }
     if (threadIdx.x == 0) {
         h->nr = nr;

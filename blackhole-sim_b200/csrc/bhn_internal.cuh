@@ -48,13 +48,15 @@ struct TableHeader {  // 128 bytes, at offset 0 of the tables buffer
     int32_t kind_r, kind_t, kind_p, pad1;
     // First guess f = X * inv - off with X = x (uniform) or X = log(x) (geometric).
     double off_r, inv_r, off_t, inv_t, off_p, inv_p;
-    double pad2[6];
+    float foff_r, finv_r, foff_t, finv_t, foff_p, finv_p;  // the same in float
+    double pad2[3];
 };
 static_assert(sizeof(TableHeader) == 128, "table header size");
 
-// Offsets (bytes) inside the tables buffer.
+// Offsets (bytes) inside the tables buffer: float64 knots, float32 reciprocal
+// spacings, float32 knots (the FP32 kernel's copy).
 struct TableLayout {
-    int64_t gr, gt, gp, idr, idt, idp, total;
+    int64_t gr, gt, gp, idr, idt, idp, grf, gtf, gpf, total;
 };
 __host__ __device__ inline TableLayout table_layout(int32_t nr, int32_t nt, int32_t np) {
     TableLayout L;
@@ -64,7 +66,10 @@ __host__ __device__ inline TableLayout table_layout(int32_t nr, int32_t nt, int3
     L.idr = L.gp + 8 * (int64_t)np;
     L.idt = L.idr + 4 * (int64_t)nr;
     L.idp = L.idt + 4 * (int64_t)nt;
-    L.total = (L.idp + 4 * (int64_t)np + 15) & ~(int64_t)15;
+    L.grf = L.idp + 4 * (int64_t)np;
+    L.gtf = L.grf + 4 * (int64_t)nr;
+    L.gpf = L.gtf + 4 * (int64_t)nt;
+    L.total = (L.gpf + 4 * (int64_t)np + 15) & ~(int64_t)15;
     return L;
 }
 
@@ -72,6 +77,7 @@ struct Tables {
     const TableHeader *h;
     const double *gr, *gt, *gp;
     const float *idr, *idt, *idp;  // 1 / (g[i+1] - g[i]); idp[np-1] spans the wrap segment
+    const float *grf, *gtf, *gpf;
 };
 __host__ __device__ inline Tables tables_at(const void *base, int32_t nr, int32_t nt, int32_t np) {
     TableLayout L = table_layout(nr, nt, np);
@@ -84,11 +90,15 @@ __host__ __device__ inline Tables tables_at(const void *base, int32_t nr, int32_
     t.idr = reinterpret_cast<const float *>(b + L.idr);
     t.idt = reinterpret_cast<const float *>(b + L.idt);
     t.idp = reinterpret_cast<const float *>(b + L.idp);
+    t.grf = reinterpret_cast<const float *>(b + L.grf);
+    t.gtf = reinterpret_cast<const float *>(b + L.gtf);
+    t.gpf = reinterpret_cast<const float *>(b + L.gpf);
     return t;
 }
 
-// lib.rs:61-73 search_right (first index with grid value > x) over [lo, hi).
-__device__ __forceinline__ int search_right(const double *g, int lo, int hi, double x) {
+// First index in [lo, hi) whose knot is > x (lib.rs:61-73 search_right).
+template <typename T>
+__device__ __forceinline__ int search_right(const T *g, int lo, int hi, T x) {
     while (lo < hi) {
         int mid = (lo + hi) >> 1;
         if (x < g[mid]) hi = mid;
@@ -129,6 +139,35 @@ __device__ __forceinline__ int locate_phi(const double *g, int n, double p, int 
     return i;
 }
 
+// The FP32 kernel's locators: the same searches over the float32 knots (exact
+// for the float32 midpoints the FP32 kernel samples at).
+__device__ __forceinline__ int locate_linear_f(const float *g, int n, float x, int kind, float off, float inv) {
+    int i;
+    if (kind == kSearch) {
+        i = search_right(g, 0, n, x) - 1;
+    } else {
+        const float f = kind == kUniform ? fmaf(x, inv, -off) : fmaf(__logf(x), inv, -off);
+        i = (int)fmaxf(f, 0.0f);
+    }
+    i = max(0, min(i, n - 2));
+    while (i > 0 && x < g[i]) --i;
+    while (i < n - 2 && x >= g[i + 1]) ++i;
+    return i;
+}
+
+__device__ __forceinline__ int locate_phi_f(const float *g, int n, float p, int kind, float off, float inv) {
+    int i;
+    if (kind == kSearch) {
+        i = search_right(g, 0, n, p) - 1;
+    } else {
+        i = (int)fmaxf(fmaf(p, inv, -off), 0.0f);
+    }
+    i = max(0, min(i, n - 1));
+    while (i > 0 && p < g[i]) --i;
+    while (i < n - 1 && p >= g[i + 1]) ++i;
+    return i;
+}
+
 // native_kernels.py:133-134 / lib.rs:89-91: ((phi - base) mod 2 pi) + base.
 __device__ __forceinline__ double wrap_phi(double phi, double base) {
     double m = fmod(phi - base, kTwoPi);
@@ -144,11 +183,11 @@ struct __align__(16) ViewDev {
     double e_r, e_th, e_ph;            // ZAMO tetrad scalings (kerr.py:144-148)
     double gcov00, gcov03, gcov11, gcov22, gcov33;
     double gcon00, gcon03, gcon11, gcon22, gcon33;
-    double r_capture, escape_radius, r_plus, r_minus;
+    double r_capture, escape_radius, r_plus, r_minus, r_photon;  // r_photon: innermost photon orbit
     double h_scale, h_min, h_max, L, max_tau;
     double width_d, height_d;          // image size as doubles (divisors of accelerated_renderer.py:138-140)
     int32_t width, height, x0, y0, crop_w, crop_h, max_steps, has_roll;
-    int32_t valid, pad[3];
+    int32_t valid, flags, pad[2];
     int64_t out_offset, ray_begin, ray_count, pad2;
 };
 

@@ -89,6 +89,10 @@ __global__ void setup_views_kernel(const bhn_view *__restrict__ raw, int n, View
         d.r_plus = 1.0 + sqrt(1.0 - a * a);   // kerr.py:39-42
         d.r_minus = 1.0 - sqrt(1.0 - a * a);
         d.r_capture = d.r_plus * (1.0 + 2.0e-4);  // kerr.py:371
+        // prograde equatorial circular photon orbit, r = 2 (1 + cos(2/3 arccos(-|a|))) (Bardeen, Press &
+        // Teukolsky 1972): the innermost spherical photon orbit, inside which an inbound ray cannot turn
+        d.r_photon = 2.0 * (1.0 + cos((2.0 / 3.0) * acos(-fabs(a))));
+        d.flags = v.flags;
         d.escape_radius = v.escape_radius;
         d.h_scale = v.h_scale;
         d.h_min = v.h_min;
@@ -179,9 +183,20 @@ __device__ __forceinline__ CameraRay camera_ray(const ViewDev &v, int px, int py
     return c;
 }
 
-struct LaneCounters {
-    unsigned long long steps, brick;
-    uint32_t rays, status[5];
+// Per-view constants of the step loop, staged in shared memory (one entry per
+// view; a lane keeps only its view index in registers).
+struct __align__(16) StepConst {
+    float a, a2, dpm, hs;               // spin, spin^2, r+ - r-, step scale
+    float hmin, hmax, L, max_tau;
+    float rp_h, rp_l, rcap_h, rcap_l;   // r+ and the capture radius as float pairs (value = hi + lo)
+    float esc, r_guard, r_near, pad;    // escape radius, horizon-guard radius (0 = off), FP64-island radius
+    int max_steps, pad1, pad2, pad3;
+};
+
+// Launch totals of one block, in shared memory (updated once per finished ray).
+struct BlockCounters {
+    unsigned long long steps, brick, fetches;
+    unsigned int rays, status[5];
     float max_drift, max_drift_escaped;
 };
 
@@ -211,247 +226,15 @@ __device__ __forceinline__ int find_view(const int64_t *begin, int n, int64_t sl
     return lo;
 }
 
-// ------------------------------------------------------------ FP32 tracer
-// sin and cos on [0, pi/2] by their Taylor series (through x^11 and x^12; the
-// truncation error is below 6e-8 at pi/2), evaluated by Horner in x^2.
-__device__ __forceinline__ void sincos_quadrant(float x, float &s, float &c) {
-    const float u = x * x;
-    float ps = fmaf(u, -2.5052108385e-8f, 2.7557319224e-6f);  // -1/11!, 1/9!
-    ps = fmaf(u, ps, -1.9841269841e-4f);                        // -1/7!
-    ps = fmaf(u, ps, 8.3333333333e-3f);                         // 1/5!
-    ps = fmaf(u, ps, -1.6666666667e-1f);                        // -1/3!
-    s = fmaf(x * u, ps, x);
-    float pc = fmaf(u, 2.0876756988e-9f, -2.7557319224e-7f);    // 1/12!, -1/10!
-    pc = fmaf(u, pc, 2.4801587302e-5f);                         // 1/8!
-    pc = fmaf(u, pc, -1.3888888889e-3f);                        // -1/6!
-    pc = fmaf(u, pc, 4.1666666667e-2f);                         // 1/4!
-    pc = fmaf(u, pc, -0.5f);                                    // -1/2!
-    c = fmaf(u, pc, 1.0f);
+// v as an unevaluated float pair hi + lo (hi = v rounded, lo = the remainder).
+__device__ __forceinline__ void split(double v, float &hi, float &lo) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
 }
 
-// sin and cos of a clamped theta from its FP64 pole distance, so that sin is
-// relatively accurate next to either pole (the near-pole metric inverse).
-__device__ __forceinline__ void pole_sincos(double th, float &s, float &c) {
-    const bool south = th > 1.5707963267948966;
-    const float d = (float)(south ? kPi - th : th);
-    sincos_quadrant(d, s, c);
-    c = south ? -c : c;
-    s = fmaxf(s, 1.0e-7f);  // s^2 >= eps^2 as kerr.py:93
-}
+constexpr double kNearHorizon = 0.1;  // FP64 island: steps that start within 0.1 M of r+
 
-struct Deriv32 {
-    float r, th, ph, pr, pth, H;
-};
-
-// Hamiltonian equations of kerr.py:285-303 written through
-//   2 Sigma H = Delta p_r^2 + p_theta^2 + P^2 - W^2 / Delta,
-//   P = p_phi / sin + a sin p_t,  W = (r^2 + a^2) p_t + a p_phi,
-// which is g^{mu nu} p_mu p_nu of kerr.py:86-102 regrouped; x' = dH/dp and
-// p' = -dH/dx are its exact derivatives (the quotient-rule sums of
-// kerr.py:236-282 collapse to these few terms).
-//
-// Delta is evaluated as (r - r+)(r - r-) from the FP64 horizon distance
-// r - r+: the expanded r^2 - 2r + a^2 cancels to nothing in FP32 within ~1e-7
-// of the horizon, where 1/Delta then overflows (the horizon-proximity FP64
-// island).
-__device__ __forceinline__ void rhs32(double rd, double r_plus, float dpm, float s, float c, float pr, float pth,
-                                      float pt, float pphi, float a, float a2, Deriv32 &d) {
-    const float r = (float)rd;
-    const float x = (float)(rd - r_plus);
-    const float r2 = r * r;
-    const float D = x * (x + dpm);
-    const float Sg = fmaf(a2 * c, c, r2);
-    const float iS = 1.0f / Sg;
-    const float iD = 1.0f / D;
-    const float is = 1.0f / s;
-    const float W = fmaf(r2 + a2, pt, a * pphi);
-    const float P = fmaf(a * s, pt, pphi * is);
-    const float Q = W * iD;
-    const float F = fmaf(D * pr, pr, fmaf(pth, pth, fmaf(P, P, -W * Q)));
-    d.r = D * pr * iS;
-    d.th = pth * iS;
-    d.ph = fmaf(P, is, -a * Q) * iS;
-    const float dFr = fmaf(2.0f * r - 2.0f, fmaf(pr, pr, Q * Q), -4.0f * r * pt * Q);
-    d.pr = fmaf(-0.5f, dFr, F * r * iS) * iS;
-    const float dFth = 2.0f * P * c * fmaf(a, pt, -pphi * is * is);
-    d.pth = fmaf(-0.5f, dFth, -F * a2 * s * c * iS) * iS;
-    d.H = 0.5f * F * iS;
-}
-
-struct Tracer32 {
-    double r, th, ph;
-    float pr, pth, pt, pphi, a, a2, dpm;
-    float S0, S1, S2, S3, tau, drift, H0;
-    float hs, hmin, hmax, L, max_tau;
-    double r_cap, esc, r_plus;
-    int steps, brick, max_steps;
-    bool poison;
-    int64_t out_idx;
-
-    __device__ __forceinline__ void init(const ViewDev &v, int px, int py, int64_t out_index) {
-        CameraRay c = camera_ray(v, px, py);
-        r = v.r_obs;
-        th = v.theta_obs;
-        ph = v.phi_obs;
-        pr = (float)c.pr;
-        pth = (float)c.pth;
-        pt = (float)c.pt;
-        pphi = (float)c.pphi;
-        a = (float)v.a;
-        a2 = a * a;
-        r_plus = v.r_plus;
-        dpm = (float)(v.r_plus - v.r_minus);
-        H0 = (float)c.H0;
-        S0 = S1 = S2 = S3 = 0.0f;
-        tau = 0.0f;
-        drift = 0.0f;
-        hs = (float)v.h_scale;
-        hmin = (float)v.h_min;
-        hmax = (float)v.h_max;
-        L = (float)v.L;
-        max_tau = (float)v.max_tau;
-        r_cap = v.r_capture;
-        esc = v.escape_radius;
-        steps = 0;
-        brick = 0;
-        max_steps = v.max_steps;
-        poison = false;
-        out_idx = out_index;
-    }
-
-    // One RK2 geodesic step plus its brick segment.  Returns -1 while the ray
-    // lives, else its BHN_RAY_* status.
-    __device__ __forceinline__ int step(const Tables &T, const float4 *__restrict__ rec, int nt, int np) {
-        const float rf = (float)r;
-        const float h = fminf(fmaxf(hs * rf, hmin), hmax);
-        float s, c;
-        pole_sincos(th, s, c);
-        Deriv32 k1;
-        rhs32(r, r_plus, dpm, s, c, pr, pth, pt, pphi, a, a2, k1);
-        drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
-        const float hh = 0.5f * h;
-        const double rm = r + (double)(hh * k1.r);
-        const double thm = safe_theta(th + (double)(hh * k1.th));
-        pole_sincos(thm, s, c);
-        Deriv32 k2;
-        rhs32(rm, r_plus, dpm, s, c, fmaf(hh, k1.pr, pr), fmaf(hh, k1.pth, pth), pt, pphi, a, a2, k2);
-        const float dr = h * k2.r, dph = h * k2.ph;
-        const double rn = r + (double)dr;
-        const double thn = safe_theta(th + (double)(h * k2.th));
-        const double phn = ph + (double)dph;
-        pr = fmaf(h, k2.pr, pr);
-        pth = fmaf(h, k2.pth, pth);
-        ++steps;
-        const bool finite = isfinite(rn) && isfinite(thn) && isfinite(phn) && isfinite(pr) && isfinite(pth);
-
-        // segment (y, y_n): accelerated_renderer.py:113-125
-        if (tau < max_tau) {
-            const double rmid = 0.5 * (r + rn), tmid = 0.5 * (th + thn), pmid = 0.5 * (ph + phn);
-            const TableHeader &H = *T.h;
-            if (!(rmid < T.gr[0] || rmid > T.gr[T.h->nr - 1]) && !(tmid < T.gt[0] || tmid > T.gt[nt - 1])) {
-                ++brick;
-                if (isnan(rmid) || isnan(tmid) || !isfinite(pmid)) {
-                    poison = true;  // NaN coefficients in the reference -> nan_to_num -> 0
-                } else {
-                    const int nr = T.h->nr;
-                    const int ir = locate_linear(T.gr, nr, rmid, H.kind_r, H.off_r, H.inv_r);
-                    const int it = locate_linear(T.gt, nt, tmid, H.kind_t, H.off_t, H.inv_t);
-                    const double pw = wrap_phi(pmid, T.gp[0]);
-                    const int ip = locate_phi(T.gp, np, pw, H.kind_p, H.off_p, H.inv_p);
-                    const int ip1 = ip + 1 == np ? 0 : ip + 1;
-                    const float wr = (float)(rmid - T.gr[ir]) * T.idr[ir];
-                    const float wt = (float)(tmid - T.gt[it]) * T.idt[it];
-                    const float wp = (float)((pw >= T.gp[ip] ? pw : pw + kTwoPi) - T.gp[ip]) * T.idp[ip];
-                    const float owr = 1.0f - wr, owt = 1.0f - wt, owp = 1.0f - wp;
-                    const int64_t c00 = ((int64_t)ir * nt + it) * np;
-                    const int64_t cells[4] = {c00, c00 + np, c00 + (int64_t)nt * np, c00 + (int64_t)nt * np + np};
-                    const float wrt[4] = {owr * owt, owr * wt, wr * owt, wr * wt};
-                    float cf[12];
-#pragma unroll
-                    for (int k = 0; k < 12; ++k) cf[k] = 0.0f;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float4 *p0 = rec + 3 * (cells[q] + ip);
-                        const float4 *p1 = rec + 3 * (cells[q] + ip1);
-                        const float w0 = wrt[q] * owp, w1 = wrt[q] * wp;
-                        const float4 a0 = __ldg(p0), b0 = __ldg(p0 + 1), c0 = __ldg(p0 + 2);
-                        const float4 a1 = __ldg(p1), b1 = __ldg(p1 + 1), c1 = __ldg(p1 + 2);
-                        cf[0] = fmaf(w0, a0.x, fmaf(w1, a1.x, cf[0]));
-                        cf[1] = fmaf(w0, a0.y, fmaf(w1, a1.y, cf[1]));
-                        cf[2] = fmaf(w0, a0.z, fmaf(w1, a1.z, cf[2]));
-                        cf[3] = fmaf(w0, a0.w, fmaf(w1, a1.w, cf[3]));
-                        cf[4] = fmaf(w0, b0.x, fmaf(w1, b1.x, cf[4]));
-                        cf[5] = fmaf(w0, b0.y, fmaf(w1, b1.y, cf[5]));
-                        cf[6] = fmaf(w0, b0.z, fmaf(w1, b1.z, cf[6]));
-                        cf[7] = fmaf(w0, b0.w, fmaf(w1, b1.w, cf[7]));
-                        cf[8] = fmaf(w0, c0.x, fmaf(w1, c1.x, cf[8]));
-                        cf[9] = fmaf(w0, c0.y, fmaf(w1, c1.y, cf[9]));
-                        cf[10] = fmaf(w0, c0.z, fmaf(w1, c1.z, cf[10]));
-                    }
-                    // ds = L * max(|d(r, theta, phi)|, 1e-14) (accelerated_renderer.py:120-121)
-                    const float dth = (float)(thn - th);
-                    const float len = sqrtf(fmaf(dr, dr, fmaf(dth, dth, dph * dph)));
-                    const float ds = L * fmaxf(len, 1.0e-14f);
-                    // Stokes RK2 (lib.rs:210-225) with K of native_kernels.py:213-222
-                    const float j0 = cf[0], j1 = cf[1], j2 = cf[2], j3 = cf[3];
-                    const float ai = cf[4], aq = cf[5], au = cf[6], av = cf[7];
-                    const float rv = cf[8], rq = cf[9], ru = cf[10];
-                    float k0 = j0 - (ai * S0 + aq * S1 + au * S2 + av * S3);
-                    float k1q = j1 - (aq * S0 + ai * S1 + rv * S2 - ru * S3);
-                    float k2u = j2 - (au * S0 - rv * S1 + ai * S2 + rq * S3);
-                    float k3v = j3 - (av * S0 + ru * S1 - rq * S2 + ai * S3);
-                    const float hd = 0.5f * ds;
-                    const float m0 = fmaf(hd, k0, S0), m1 = fmaf(hd, k1q, S1), m2 = fmaf(hd, k2u, S2),
-                                m3 = fmaf(hd, k3v, S3);
-                    k0 = j0 - (ai * m0 + aq * m1 + au * m2 + av * m3);
-                    k1q = j1 - (aq * m0 + ai * m1 + rv * m2 - ru * m3);
-                    k2u = j2 - (au * m0 - rv * m1 + ai * m2 + rq * m3);
-                    k3v = j3 - (av * m0 + ru * m1 - rq * m2 + ai * m3);
-                    S0 = fmaf(ds, k0, S0);
-                    S1 = fmaf(ds, k1q, S1);
-                    S2 = fmaf(ds, k2u, S2);
-                    S3 = fmaf(ds, k3v, S3);
-                    tau = fmaf(fmaxf(ai, 0.0f), ds, tau);
-                }
-            }
-        }
-        const double r_old = r;
-        r = rn;
-        th = thn;
-        ph = phn;
-        // kerr.py:364-377, in FP64
-        if (!finite) return BHN_RAY_INVALID;
-        if (tau >= max_tau) return BHN_RAY_OPAQUE;
-        if (rn <= r_cap) return BHN_RAY_CAPTURED;
-        if (rn > esc && rn > r_old) return BHN_RAY_ESCAPED;
-        if (steps >= max_steps) return BHN_RAY_MAX_STEPS;
-        return -1;
-    }
-
-    __device__ __forceinline__ void finish(void *out, int status) {
-        // drift at the final state (kerr.py:360, 367)
-        if (status != BHN_RAY_INVALID) {
-            float s, c;
-            pole_sincos(th, s, c);
-            Deriv32 k;
-            rhs32(r, r_plus, dpm, s, c, pr, pth, pt, pphi, a, a2, k);
-            drift = fmaxf(drift, fabsf(fabsf(k.H) - H0));
-        }
-        float4 o;
-        // np.nan_to_num(S, nan=0, posinf=0, neginf=0) (accelerated_renderer.py:126)
-        o.x = (poison || !isfinite(S0)) ? 0.0f : S0;
-        o.y = (poison || !isfinite(S1)) ? 0.0f : S1;
-        o.z = (poison || !isfinite(S2)) ? 0.0f : S2;
-        o.w = (poison || !isfinite(S3)) ? 0.0f : S3;
-        reinterpret_cast<float4 *>(out)[out_idx] = o;
-    }
-
-    static __device__ __forceinline__ void write_zero(void *out, int64_t idx) {
-        reinterpret_cast<float4 *>(out)[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-};
-
-// ------------------------------------------------------------ FP64 tracer
+// ------------------------------------------------------------ FP64 helpers
 // kerr.py:52-64, :86-102, :236-303 in FP64 (the oracle's formulation).
 struct Metric64 {
     double g00, g03, g11, g22, g33;
@@ -526,16 +309,349 @@ __device__ __forceinline__ void rhs64(double r, double th_in, double pr, double 
     d.H = 0.5 * quad64(g, pt, pr, pth, pphi);
 }
 
-struct Tracer64 {
-    double r, th, ph, pr, pth, pt, pphi, a;
-    double S0, S1, S2, S3, tau, drift, H0;
-    double hs, hmin, hmax, L, max_tau, r_cap, esc;
-    int steps, brick, max_steps;
-    bool poison;
-    int64_t out_idx;
+// ------------------------------------------------------------ FP32 tracer
+constexpr float kPiH = 3.14159274101257324f;        // pi rounded to float
+constexpr float kPiL = -8.74227765734758577e-8f;    // pi - kPiH
+constexpr float kHalfPiF = 1.57079637050628662f;
+constexpr float kTwoPiH = 6.28318548202514648f;     // 2 pi rounded to float
+constexpr float kTwoPiL = -1.74845553146951715e-7f; // 2 pi - kTwoPiH
+constexpr float kEpsF = 1.0e-7f;
+constexpr float kTmaxH = (float)(kPi - kEpsTheta);  // pi - eps as a float pair (kerr.py:35-36 upper clamp)
+constexpr float kTmaxL = (float)((kPi - kEpsTheta) - (double)kTmaxH);
 
-    __device__ __forceinline__ void init(const ViewDev &v, int px, int py, int64_t out_index) {
-        CameraRay c = camera_ray(v, px, py);
+// sin and cos on [0, pi/2] by their Taylor series (through x^11 and x^12; the
+// truncation error is below 6e-8 at pi/2), evaluated by Horner in x^2.
+__device__ __forceinline__ void sincos_quadrant(float x, float &s, float &c) {
+    const float u = x * x;
+    float ps = fmaf(u, -2.5052108385e-8f, 2.7557319224e-6f);  // -1/11!, 1/9!
+    ps = fmaf(u, ps, -1.9841269841e-4f);                        // -1/7!
+    ps = fmaf(u, ps, 8.3333333333e-3f);                         // 1/5!
+    ps = fmaf(u, ps, -1.6666666667e-1f);                        // -1/3!
+    s = fmaf(x * u, ps, x);
+    float pc = fmaf(u, 2.0876756988e-9f, -2.7557319224e-7f);    // 1/12!, -1/10!
+    pc = fmaf(u, pc, 2.4801587302e-5f);                         // 1/8!
+    pc = fmaf(u, pc, -1.3888888889e-3f);                        // -1/6!
+    pc = fmaf(u, pc, 4.1666666667e-2f);                         // 1/4!
+    pc = fmaf(u, pc, -0.5f);                                    // -1/2!
+    c = fmaf(u, pc, 1.0f);
+}
+
+// sin(theta), cos(theta) from d, the distance of theta from the pole nearer
+// at the step start (south: theta = pi - d).  d keeps full relative precision
+// next to either pole because it is formed from the compensated theta, which
+// is what the near-pole metric inverse (g^phiphi ~ 1/sin^2) needs.
+__device__ __forceinline__ void sincos_pole(float d, bool south, float &s, float &c) {
+    const bool over = d > kHalfPiF;  // a half step may cross the equator
+    const float x = over ? (kPiH - d) + kPiL : d;
+    sincos_quadrant(x, s, c);
+    c = (over != south) ? -c : c;
+    s = fmaxf(s, kEpsF);  // sin^2 >= eps^2 (kerr.py:93)
+}
+
+// hi + lo += d (Kahan's compensated summation: lo carries what hi lost).
+__device__ __forceinline__ void kahan_add(float &hi, float &lo, float d) {
+    const float y = d + lo;
+    const float t = hi + y;
+    lo = y - (t - hi);
+    hi = t;
+}
+
+// hi + lo += d without the |hi| >= |d| precondition (Knuth's TwoSum).
+__device__ __forceinline__ void two_sum_add(float &hi, float &lo, float d) {
+    const float s = hi + d;
+    const float bb = s - hi;
+    const float err = (hi - (s - bb)) + (d - bb);
+    hi = s;
+    lo += err;
+}
+
+struct Deriv32 {
+    float r, th, ph, pr, pth, H;
+};
+
+// Hamiltonian equations of kerr.py:285-303 written through
+//   2 Sigma H = Delta p_r^2 + p_theta^2 + P^2 - W^2 / Delta,
+//   P = p_phi / sin + a sin p_t,  W = (r^2 + a^2) p_t + a p_phi,
+// which is g^{mu nu} p_mu p_nu of kerr.py:86-102 regrouped; x' = dH/dp and
+// p' = -dH/dx are its exact derivatives (the quotient-rule sums of
+// kerr.py:236-282 collapse to these few terms).  Delta is formed as
+// (r - r+)(r - r-) from the compensated horizon distance x = r - r+, since
+// r^2 - 2r + a^2 cancels to nothing in FP32 next to the horizon.
+__device__ __forceinline__ void rhs32(float r, float x, float s, float c, float pr, float pth, float pt, float pphi,
+                                      float a, float a2, float dpm, Deriv32 &d) {
+    const float r2 = r * r;
+    const float D = x * (x + dpm);
+    const float Sg = fmaf(a2 * c, c, r2);
+    const float iS = 1.0f / Sg;
+    const float iD = 1.0f / D;
+    const float is = 1.0f / s;
+    const float W = fmaf(r2 + a2, pt, a * pphi);
+    const float P = fmaf(a * s, pt, pphi * is);
+    const float Q = W * iD;
+    const float F = fmaf(D * pr, pr, fmaf(pth, pth, fmaf(P, P, -W * Q)));
+    d.r = D * pr * iS;
+    d.th = pth * iS;
+    d.ph = fmaf(P, is, -a * Q) * iS;
+    const float dFr = fmaf(2.0f * r - 2.0f, fmaf(pr, pr, Q * Q), -4.0f * r * pt * Q);
+    d.pr = fmaf(-0.5f, dFr, F * r * iS) * iS;
+    const float dFth = 2.0f * P * c * fmaf(a, pt, -pphi * is * is);
+    d.pth = fmaf(-0.5f, dFth, -F * a2 * s * c * iS) * iS;
+    d.H = 0.5f * F * iS;
+}
+
+// rhs32's Hamiltonian form in FP64 (the near-horizon island of the FP32 kernel).
+__device__ __forceinline__ void rhs64h(double r, double th_in, double pr, double pth, double pt, double pphi,
+                                       double a, double r_plus, double r_minus, Deriv64 &d) {
+    const double th = safe_theta(th_in);
+    double s, c;
+    sincos(th, &s, &c);
+    s = fmax(s, kEpsTheta);
+    const double a2 = a * a, r2 = r * r;
+    const double D = (r - r_plus) * (r - r_minus);
+    const double Sg = r2 + a2 * c * c;
+    const double iS = 1.0 / Sg, iD = 1.0 / D, is = 1.0 / s;
+    const double W = (r2 + a2) * pt + a * pphi;
+    const double P = pphi * is + a * s * pt;
+    const double Q = W * iD;
+    const double F = D * pr * pr + pth * pth + P * P - W * Q;
+    d.r = D * pr * iS;
+    d.th = pth * iS;
+    d.ph = (P * is - a * Q) * iS;
+    const double dFr = (2.0 * r - 2.0) * (pr * pr + Q * Q) - 4.0 * r * pt * Q;
+    d.pr = (-0.5 * dFr + F * r * iS) * iS;
+    const double dFth = 2.0 * P * c * (a * pt - pphi * is * is);
+    d.pth = (-0.5 * dFth - F * a2 * s * c * iS) * iS;
+    d.H = 0.5 * F * iS;
+}
+
+struct Tracer32 {
+    float rh, rl, th_h, th_l, ph_h, ph_l;  // positions as compensated pairs (value = hi + lo)
+    float pr, pth, pt, pphi;
+    float S0, S1, S2, S3, tau, drift, H0;
+    int steps, brick, vi;
+    uint32_t out_idx;
+
+    __device__ __forceinline__ void init(const ViewDev &v, int view, int px, int py, int64_t out_index) {
+        const CameraRay c = camera_ray(v, px, py);
+        split(v.r_obs, rh, rl);
+        split(v.theta_obs, th_h, th_l);
+        double p0 = fmod(v.phi_obs, kTwoPi);
+        if (p0 < 0.0) p0 += kTwoPi;
+        split(p0, ph_h, ph_l);
+        pr = (float)c.pr;
+        pth = (float)c.pth;
+        pt = (float)c.pt;
+        pphi = (float)c.pphi;
+        H0 = (float)c.H0;
+        S0 = S1 = S2 = S3 = 0.0f;
+        tau = 0.0f;
+        drift = 0.0f;
+        steps = 0;
+        brick = 0;
+        vi = view;
+        out_idx = (uint32_t)out_index;
+    }
+
+    // The FP64 island next to the horizon: the whole RK2 step in FP64, since
+    // p_r ~ 1/Delta leaves FP32's exponent range there.
+    __device__ __forceinline__ bool step_fp64(const ViewDev &v, float &dr, float &dph) {
+        const double r = (double)rh + (double)rl;
+        const double th = (double)th_h + (double)th_l;
+        const double ph = (double)ph_h + (double)ph_l;
+        const double h = fmin(fmax(v.h_scale * r, v.h_min), v.h_max);
+        Deriv64 k1, k2;
+        rhs64h(r, th, pr, pth, pt, pphi, v.a, v.r_plus, v.r_minus, k1);
+        drift = fmaxf(drift, (float)fabs(fabs(k1.H) - (double)H0));
+        const double hh = 0.5 * h;
+        rhs64h(r + hh * k1.r, th + hh * k1.th, pr + hh * k1.pr, pth + hh * k1.pth, pt, pphi, v.a, v.r_plus,
+               v.r_minus, k2);
+        const double rn = r + h * k2.r, thn = safe_theta(th + h * k2.th), phn = ph + h * k2.ph;
+        const double prn = pr + h * k2.pr, pthn = pth + h * k2.pth;
+        dr = (float)(rn - r);
+        dph = (float)(phn - ph);
+        split(rn, rh, rl);
+        split(thn, th_h, th_l);
+        split(phn, ph_h, ph_l);
+        pr = (float)prn;
+        pth = (float)pthn;
+        return isfinite(rn) && isfinite(thn) && isfinite(phn) && isfinite(prn) && isfinite(pthn);
+    }
+
+    // One RK2 geodesic step plus its brick segment.  Returns -1 while the ray
+    // lives, else its BHN_RAY_* status.
+    __device__ __forceinline__ int step(const StepConst &C, const Tables &T, const float4 *__restrict__ rec, int nr,
+                                        int nt, int np, const ViewDev *__restrict__ views) {
+        if (rh < C.r_guard && pr < 0.0f) return BHN_RAY_CAPTURED;  // horizon guard (flag; off by default)
+        const float r0 = rh + rl, th0 = th_h + th_l, ph0 = ph_h + ph_l;
+        float dr, dph;
+        bool finite;
+        if (rh < C.r_near) {
+            finite = step_fp64(views[vi], dr, dph);
+        } else {
+            const bool south = th_h > kHalfPiF;
+            const float d0 = south ? (kPiH - th_h) + (kPiL - th_l) : th0;
+            float s, c;
+            sincos_pole(d0, south, s, c);
+            const float x0 = (rh - C.rp_h) + (rl - C.rp_l);
+            const float h = fminf(fmaxf(C.hs * r0, C.hmin), C.hmax);
+            Deriv32 k1;
+            rhs32(r0, x0, s, c, pr, pth, pt, pphi, C.a, C.a2, C.dpm, k1);
+            drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
+            const float hh = 0.5f * h;
+            // midpoint: pole distance clamped at eps like kerr.py:35-36 inside the right-hand side
+            const float dm = fmaxf(south ? fmaf(-hh, k1.th, d0) : fmaf(hh, k1.th, d0), kEpsF);
+            sincos_pole(dm, south, s, c);
+            Deriv32 k2;
+            rhs32(fmaf(hh, k1.r, r0), fmaf(hh, k1.r, x0), s, c, fmaf(hh, k1.pr, pr), fmaf(hh, k1.pth, pth), pt, pphi,
+                  C.a, C.a2, C.dpm, k2);
+            dr = h * k2.r;
+            const float dth = h * k2.th;
+            dph = h * k2.ph;
+            kahan_add(rh, rl, dr);
+            kahan_add(th_h, th_l, dth);
+            kahan_add(ph_h, ph_l, dph);
+            pr = fmaf(h, k2.pr, pr);
+            pth = fmaf(h, k2.pth, pth);
+            finite = isfinite(dr + dth + dph + pr + pth);
+            // theta clamp (kerr.py:312)
+            if (th_h + th_l < kEpsF) {
+                th_h = kEpsF;
+                th_l = 0.0f;
+            } else if ((th_h - kTmaxH) + (th_l - kTmaxL) > 0.0f) {
+                th_h = kTmaxH;
+                th_l = kTmaxL;
+            }
+        }
+        ++steps;
+        const float th1 = th_h + th_l;
+        // phi is only sampled modulo 2 pi: keep the state in [0, 2 pi)
+        if (ph_h >= kTwoPiH) {
+            two_sum_add(ph_h, ph_l, -kTwoPiH);
+            ph_l -= kTwoPiL;
+        } else if (ph_h < 0.0f) {
+            two_sum_add(ph_h, ph_l, kTwoPiH);
+            ph_l += kTwoPiL;
+        }
+
+        // segment (y, y_n): accelerated_renderer.py:113-125
+        if (tau < C.max_tau) {
+            const float rmid = fmaf(0.5f, dr, r0), tmid = 0.5f * (th0 + th1), pmid = fmaf(0.5f, dph, ph0);
+            // nonperiodic valid mask (native_kernels.py:189-210); NaN passes it as in the reference
+            if (!(rmid < T.grf[0] || rmid > T.grf[nr - 1]) && !(tmid < T.gtf[0] || tmid > T.gtf[nt - 1])) {
+                ++brick;
+                if (!(isfinite(rmid) && isfinite(tmid) && isfinite(pmid))) {
+                    // NaN coefficients in the reference -> NaN Stokes -> nan_to_num -> 0
+                    S0 = S1 = S2 = S3 = __int_as_float(0x7fc00000);
+                } else {
+                    const TableHeader &H = *T.h;
+                    const float g0 = T.gpf[0];
+                    float pw = pmid - g0;
+                    pw = fmaf(-kTwoPiH, floorf(pw * 0.159154943f), pw) + g0;  // wrap into [g0, g0 + 2 pi)
+                    pw = fmaxf(pw, g0);
+                    const int ir = locate_linear_f(T.grf, nr, rmid, H.kind_r, H.foff_r, H.finv_r);
+                    const int it = locate_linear_f(T.gtf, nt, tmid, H.kind_t, H.foff_t, H.finv_t);
+                    const int ip = locate_phi_f(T.gpf, np, pw, H.kind_p, H.foff_p, H.finv_p);
+                    const int ip1 = ip + 1 == np ? 0 : ip + 1;
+                    const float wr = (rmid - T.grf[ir]) * T.idr[ir];
+                    const float wt = (tmid - T.gtf[it]) * T.idt[it];
+                    const float wp = (pw - T.gpf[ip]) * T.idp[ip];
+                    const float owr = 1.0f - wr, owt = 1.0f - wt, owp = 1.0f - wp;
+                    const int64_t c00 = ((int64_t)ir * nt + it) * np;
+                    const int64_t cells[4] = {c00, c00 + np, c00 + (int64_t)nt * np, c00 + (int64_t)nt * np + np};
+                    const float wrt[4] = {owr * owt, owr * wt, wr * owt, wr * wt};
+                    float cf[11];
+#pragma unroll
+                    for (int k = 0; k < 11; ++k) cf[k] = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float4 *p0 = rec + 3 * (cells[q] + ip);
+                        const float4 *p1 = rec + 3 * (cells[q] + ip1);
+                        const float w0 = wrt[q] * owp, w1 = wrt[q] * wp;
+                        const float4 a0 = __ldg(p0), b0 = __ldg(p0 + 1), c0 = __ldg(p0 + 2);
+                        const float4 a1 = __ldg(p1), b1 = __ldg(p1 + 1), c1 = __ldg(p1 + 2);
+                        cf[0] = fmaf(w0, a0.x, fmaf(w1, a1.x, cf[0]));
+                        cf[1] = fmaf(w0, a0.y, fmaf(w1, a1.y, cf[1]));
+                        cf[2] = fmaf(w0, a0.z, fmaf(w1, a1.z, cf[2]));
+                        cf[3] = fmaf(w0, a0.w, fmaf(w1, a1.w, cf[3]));
+                        cf[4] = fmaf(w0, b0.x, fmaf(w1, b1.x, cf[4]));
+                        cf[5] = fmaf(w0, b0.y, fmaf(w1, b1.y, cf[5]));
+                        cf[6] = fmaf(w0, b0.z, fmaf(w1, b1.z, cf[6]));
+                        cf[7] = fmaf(w0, b0.w, fmaf(w1, b1.w, cf[7]));
+                        cf[8] = fmaf(w0, c0.x, fmaf(w1, c1.x, cf[8]));
+                        cf[9] = fmaf(w0, c0.y, fmaf(w1, c1.y, cf[9]));
+                        cf[10] = fmaf(w0, c0.z, fmaf(w1, c1.z, cf[10]));
+                    }
+                    // ds = L * max(|d(r, theta, phi)|, 1e-14) (accelerated_renderer.py:120-121)
+                    const float dth = th1 - th0;
+                    const float ds = C.L * fmaxf(sqrtf(fmaf(dr, dr, fmaf(dth, dth, dph * dph))), 1.0e-14f);
+                    // Stokes RK2 (lib.rs:210-225) with K of native_kernels.py:213-222
+                    const float j0 = cf[0], j1 = cf[1], j2 = cf[2], j3 = cf[3];
+                    const float ai = cf[4], aq = cf[5], au = cf[6], av = cf[7];
+                    const float rv = cf[8], rq = cf[9], ru = cf[10];
+                    float k0 = j0 - (ai * S0 + aq * S1 + au * S2 + av * S3);
+                    float kq = j1 - (aq * S0 + ai * S1 + rv * S2 - ru * S3);
+                    float ku = j2 - (au * S0 - rv * S1 + ai * S2 + rq * S3);
+                    float kv = j3 - (av * S0 + ru * S1 - rq * S2 + ai * S3);
+                    const float hd = 0.5f * ds;
+                    const float m0 = fmaf(hd, k0, S0), m1 = fmaf(hd, kq, S1), m2 = fmaf(hd, ku, S2),
+                                m3 = fmaf(hd, kv, S3);
+                    k0 = j0 - (ai * m0 + aq * m1 + au * m2 + av * m3);
+                    kq = j1 - (aq * m0 + ai * m1 + rv * m2 - ru * m3);
+                    ku = j2 - (au * m0 - rv * m1 + ai * m2 + rq * m3);
+                    kv = j3 - (av * m0 + ru * m1 - rq * m2 + ai * m3);
+                    S0 = fmaf(ds, k0, S0);
+                    S1 = fmaf(ds, kq, S1);
+                    S2 = fmaf(ds, ku, S2);
+                    S3 = fmaf(ds, kv, S3);
+                    tau = fmaf(fmaxf(ai, 0.0f), ds, tau);
+                }
+            }
+        }
+        // kerr.py:364-377
+        if (!finite) return BHN_RAY_INVALID;
+        if (tau >= C.max_tau) return BHN_RAY_OPAQUE;
+        if ((rh - C.rcap_h) + (rl - C.rcap_l) <= 0.0f) return BHN_RAY_CAPTURED;
+        if (rh > C.esc && dr > 0.0f) return BHN_RAY_ESCAPED;
+        if (steps >= C.max_steps) return BHN_RAY_MAX_STEPS;
+        return -1;
+    }
+
+    __device__ __forceinline__ void finish(void *out, int status, const StepConst &C, const ViewDev *) {
+        if (status != BHN_RAY_INVALID) {  // drift at the final state (kerr.py:360, 367)
+            const bool south = th_h > kHalfPiF;
+            const float d0 = south ? (kPiH - th_h) + (kPiL - th_l) : th_h + th_l;
+            float s, c;
+            sincos_pole(d0, south, s, c);
+            Deriv32 k;
+            rhs32(rh + rl, (rh - C.rp_h) + (rl - C.rp_l), s, c, pr, pth, pt, pphi, C.a, C.a2, C.dpm, k);
+            drift = fmaxf(drift, fabsf(fabsf(k.H) - H0));
+        }
+        // np.nan_to_num(S, nan=0, posinf=0, neginf=0) (accelerated_renderer.py:126)
+        float4 o;
+        o.x = isfinite(S0) ? S0 : 0.0f;
+        o.y = isfinite(S1) ? S1 : 0.0f;
+        o.z = isfinite(S2) ? S2 : 0.0f;
+        o.w = isfinite(S3) ? S3 : 0.0f;
+        reinterpret_cast<float4 *>(out)[out_idx] = o;
+    }
+
+    __device__ __forceinline__ float drift_f() const { return drift; }
+
+    static __device__ __forceinline__ void write_zero(void *out, int64_t idx) {
+        reinterpret_cast<float4 *>(out)[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+};
+
+// ------------------------------------------------------------ FP64 tracer
+struct Tracer64 {
+    double r, th, ph, pr, pth, pt, pphi;
+    double S0, S1, S2, S3, tau, drift, H0;
+    int steps, brick, vi;
+    bool poison;
+    uint32_t out_idx;
+
+    __device__ __forceinline__ void init(const ViewDev &v, int view, int px, int py, int64_t out_index) {
+        const CameraRay c = camera_ray(v, px, py);
         r = v.r_obs;
         th = v.theta_obs;
         ph = v.phi_obs;
@@ -543,32 +659,27 @@ struct Tracer64 {
         pth = c.pth;
         pt = c.pt;
         pphi = c.pphi;
-        a = v.a;
         H0 = c.H0;
         S0 = S1 = S2 = S3 = 0.0;
         tau = 0.0;
         drift = 0.0;
-        hs = v.h_scale;
-        hmin = v.h_min;
-        hmax = v.h_max;
-        L = v.L;
-        max_tau = v.max_tau;
-        r_cap = v.r_capture;
-        esc = v.escape_radius;
         steps = 0;
         brick = 0;
-        max_steps = v.max_steps;
+        vi = view;
         poison = false;
-        out_idx = out_index;
+        out_idx = (uint32_t)out_index;
     }
 
-    __device__ __forceinline__ int step(const Tables &T, const double2 *__restrict__ rec, int nt, int np) {
-        const double h = fmin(fmax(hs * r, hmin), hmax);
+    __device__ __forceinline__ int step(const StepConst &C, const Tables &T, const double2 *__restrict__ rec, int nr,
+                                        int nt, int np, const ViewDev *__restrict__ views) {
+        const ViewDev &v = views[vi];
+        if (C.r_guard > 0.0f && r < fmin(v.r_photon, T.gr[0]) && pr < 0.0) return BHN_RAY_CAPTURED;
+        const double h = fmin(fmax(v.h_scale * r, v.h_min), v.h_max);
         Deriv64 k1, k2;
-        rhs64(r, th, pr, pth, pt, pphi, a, k1);
+        rhs64(r, th, pr, pth, pt, pphi, v.a, k1);
         drift = fmax(drift, fabs(fabs(k1.H) - H0));
         const double hh = 0.5 * h;
-        rhs64(r + hh * k1.r, th + hh * k1.th, pr + hh * k1.pr, pth + hh * k1.pth, pt, pphi, a, k2);
+        rhs64(r + hh * k1.r, th + hh * k1.th, pr + hh * k1.pr, pth + hh * k1.pth, pt, pphi, v.a, k2);
         const double rn = r + h * k2.r;
         const double thn = safe_theta(th + h * k2.th);
         const double phn = ph + h * k2.ph;
@@ -576,10 +687,9 @@ struct Tracer64 {
         pth = pth + h * k2.pth;
         ++steps;
         const bool finite = isfinite(rn) && isfinite(thn) && isfinite(phn) && isfinite(pr) && isfinite(pth);
-        if (tau < max_tau) {
+        if (tau < v.max_tau) {
             const double rmid = 0.5 * (r + rn), tmid = 0.5 * (th + thn), pmid = 0.5 * (ph + phn);
             const TableHeader &H = *T.h;
-            const int nr = H.nr;
             if (!(rmid < T.gr[0] || rmid > T.gr[nr - 1]) && !(tmid < T.gt[0] || tmid > T.gt[nt - 1])) {
                 ++brick;
                 if (isnan(rmid) || isnan(tmid) || !isfinite(pmid)) {
@@ -619,7 +729,7 @@ struct Tracer64 {
                     const double d0 = rn - r, d1 = thn - th, d2 = phn - ph;
                     double dl = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
                     if (1.0e-14 > dl) dl = 1.0e-14;
-                    double ds = L * dl;
+                    double ds = v.L * dl;
                     if (ds < 0.0) ds = 0.0;
                     const double j0 = cf[0], j1 = cf[1], j2 = cf[2], j3 = cf[3];
                     const double ai = cf[4], aq = cf[5], au = cf[6], av = cf[7];
@@ -647,23 +757,25 @@ struct Tracer64 {
         th = thn;
         ph = phn;
         if (!finite) return BHN_RAY_INVALID;
-        if (tau >= max_tau) return BHN_RAY_OPAQUE;
-        if (rn <= r_cap) return BHN_RAY_CAPTURED;
-        if (rn > esc && rn > r_old) return BHN_RAY_ESCAPED;
-        if (steps >= max_steps) return BHN_RAY_MAX_STEPS;
+        if (tau >= v.max_tau) return BHN_RAY_OPAQUE;
+        if (rn <= v.r_capture) return BHN_RAY_CAPTURED;
+        if (rn > v.escape_radius && rn > r_old) return BHN_RAY_ESCAPED;
+        if (steps >= v.max_steps) return BHN_RAY_MAX_STEPS;
         return -1;
     }
 
-    __device__ __forceinline__ void finish(void *out, int status) {
+    __device__ __forceinline__ void finish(void *out, int status, const StepConst &C, const ViewDev *views) {
         if (status != BHN_RAY_INVALID) {
             Deriv64 k;
-            rhs64(r, th, pr, pth, pt, pphi, a, k);
+            rhs64(r, th, pr, pth, pt, pphi, views[vi].a, k);
             drift = fmax(drift, fabs(fabs(k.H) - H0));
         }
-        double2 *o = reinterpret_cast<double2 *>(out) + 2 * out_idx;
+        double2 *o = reinterpret_cast<double2 *>(out) + 2 * (int64_t)out_idx;
         o[0] = make_double2((poison || !isfinite(S0)) ? 0.0 : S0, (poison || !isfinite(S1)) ? 0.0 : S1);
         o[1] = make_double2((poison || !isfinite(S2)) ? 0.0 : S2, (poison || !isfinite(S3)) ? 0.0 : S3);
     }
+
+    __device__ __forceinline__ float drift_f() const { return (float)drift; }
 
     static __device__ __forceinline__ void write_zero(void *out, int64_t idx) {
         double2 *o = reinterpret_cast<double2 *>(out) + 2 * idx;
@@ -676,21 +788,55 @@ template <class T> struct RecordOf;
 template <> struct RecordOf<Tracer32> { using type = float4; };
 template <> struct RecordOf<Tracer64> { using type = double2; };
 
+__host__ __device__ inline int64_t align16(int64_t x) { return (x + 15) & ~(int64_t)15; }
+
+// Shared-memory layout of the persistent kernel.
+__host__ __device__ inline int64_t smem_bytes(int tables_bytes, int n_views) {
+    return align16(tables_bytes) + align16(8 * ((int64_t)n_views + 1)) + (int64_t)sizeof(StepConst) * n_views +
+           align16(sizeof(BlockCounters));
+}
+
 // ------------------------------------------------------------ persistent loop
-template <class Tracer>
-__global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
+// MINB = resident 256-thread blocks the register allocation must allow:
+// 1 -> unconstrained, 3 -> <= 85 registers, 4 -> <= 64 registers.
+template <class Tracer, int MINB>
+__global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
-    // grid tables and the view prefix live in shared memory for the whole launch
+    int64_t *vbegin = reinterpret_cast<int64_t *>(smem + align16(P.tables_bytes));
+    StepConst *sconst = reinterpret_cast<StepConst *>(smem + align16(P.tables_bytes) + align16(8 * (P.n_views + 1)));
+    BlockCounters *bc = reinterpret_cast<BlockCounters *>(sconst + P.n_views);
+    // grid tables, the view prefix and the per-view step constants stay in shared memory for the launch
     {
         const int4 *src = reinterpret_cast<const int4 *>(P.tables);
         int4 *dst = reinterpret_cast<int4 *>(smem);
         for (int i = threadIdx.x; i < P.tables_bytes / 16; i += blockDim.x) dst[i] = src[i];
-        int64_t *vb = reinterpret_cast<int64_t *>(smem + P.tables_bytes);
-        for (int i = threadIdx.x; i <= P.n_views; i += blockDim.x) vb[i] = P.ray_begin[i];
+        for (int i = threadIdx.x; i <= P.n_views; i += blockDim.x) vbegin[i] = P.ray_begin[i];
+        if (threadIdx.x == 0) memset(bc, 0, sizeof(BlockCounters));
     }
     __syncthreads();
     const Tables T = tables_at(smem, P.nr, P.nt, P.np);
-    const int64_t *vbegin = reinterpret_cast<const int64_t *>(smem + P.tables_bytes);
+    for (int i = threadIdx.x; i < P.n_views; i += blockDim.x) {
+        const ViewDev &v = P.views[i];
+        StepConst c;
+        c.a = (float)v.a;
+        c.a2 = c.a * c.a;
+        c.dpm = (float)(v.r_plus - v.r_minus);
+        c.hs = (float)v.h_scale;
+        c.hmin = (float)v.h_min;
+        c.hmax = (float)v.h_max;
+        c.L = (float)v.L;
+        c.max_tau = (float)v.max_tau;
+        split(v.r_plus, c.rp_h, c.rp_l);
+        split(v.r_capture, c.rcap_h, c.rcap_l);
+        c.esc = (float)v.escape_radius;
+        c.r_guard = (v.flags & BHN_VIEW_HORIZON_GUARD) ? (float)fmin(v.r_photon, T.gr[0]) : 0.0f;
+        c.r_near = (float)(v.r_plus + kNearHorizon);
+        c.pad = 0.0f;
+        c.max_steps = v.max_steps;
+        c.pad1 = c.pad2 = c.pad3 = 0;
+        sconst[i] = c;
+    }
+    __syncthreads();
     const unsigned long long total = vbegin[P.n_views];
     using Rec = typename RecordOf<Tracer>::type;
     const Rec *rec = reinterpret_cast<const Rec *>(P.records);
@@ -699,22 +845,17 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
     const unsigned lt_mask = (1u << lane) - 1u;
     Tracer tr;
     bool alive = false, exhausted = false;
-    LaneCounters cnt;
-    cnt.steps = cnt.brick = 0;
-    cnt.rays = 0;
-    for (int k = 0; k < 5; ++k) cnt.status[k] = 0;
-    cnt.max_drift = 0.0f;
-    cnt.max_drift_escaped = 0.0f;
-    unsigned long long fetches = 0;
 
     while (true) {
         const unsigned dead = __ballot_sync(kFull, !alive);
         const int ndead = __popc(dead);
         if (!exhausted && ndead > 0 && (ndead >= P.refill_min || ndead == 32)) {
             unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(&P.q->next, (unsigned long long)ndead);
+            if (lane == 0) {
+                base = atomicAdd(&P.q->next, (unsigned long long)ndead);
+                atomicAdd(&bc->fetches, 1ull);
+            }
             base = __shfl_sync(kFull, base, 0);
-            ++fetches;
             if (base + (unsigned long long)ndead >= total) exhausted = true;
             if (!alive) {
                 const unsigned long long slot = base + __popc(dead & lt_mask);
@@ -723,17 +864,16 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
                     const ViewDev &v = P.views[vi];
                     const PixelRef px = pixel_of(v, (int64_t)slot - vbegin[vi], P.tile_w, P.tile_h);
                     if (v.valid && v.max_steps > 0) {
-                        tr.init(v, px.px, px.py, px.out_idx);
+                        tr.init(v, vi, px.px, px.py, px.out_idx);
                         alive = true;
                     } else {
                         // no step is taken: the reference returns a zero Stokes vector
                         Tracer::write_zero(P.out, px.out_idx);
-                        cnt.rays += 1;
                         const int zst = v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID;
-#pragma unroll
-                        for (int k = 0; k < 5; ++k) cnt.status[k] += (zst == k);
+                        atomicAdd(&bc->rays, 1u);
+                        atomicAdd(&bc->status[zst], 1u);
                         if (P.ray_steps) P.ray_steps[px.out_idx] = 0;
-                        if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)(v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID);
+                        if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)zst;
                         if (P.ray_drift) P.ray_drift[px.out_idx] = 0.0f;
                     }
                 }
@@ -744,45 +884,38 @@ __global__ void __launch_bounds__(256) render_kernel(const RenderParams P) {
             continue;
         }
         if (alive) {
-            const int st = tr.step(T, rec, P.nt, P.np);
+            const StepConst &C = sconst[tr.vi];
+            const int st = tr.step(C, T, rec, P.nr, P.nt, P.np, P.views);
             if (st >= 0) {
-                tr.finish(P.out, st);
-                cnt.steps += (unsigned long long)tr.steps;
-                cnt.brick += (unsigned long long)tr.brick;
-                cnt.rays += 1;
-#pragma unroll
-                for (int k = 0; k < 5; ++k) cnt.status[k] += (st == k);
-                cnt.max_drift = fmaxf(cnt.max_drift, (float)tr.drift);
-                if (st == BHN_RAY_ESCAPED) cnt.max_drift_escaped = fmaxf(cnt.max_drift_escaped, (float)tr.drift);
+                tr.finish(P.out, st, C, P.views);
+                const float d = tr.drift_f();
+                atomicAdd(&bc->steps, (unsigned long long)tr.steps);
+                atomicAdd(&bc->brick, (unsigned long long)tr.brick);
+                atomicAdd(&bc->rays, 1u);
+                atomicAdd(&bc->status[st], 1u);
+                atomicMax(reinterpret_cast<unsigned int *>(&bc->max_drift), __float_as_uint(d));
+                if (st == BHN_RAY_ESCAPED)
+                    atomicMax(reinterpret_cast<unsigned int *>(&bc->max_drift_escaped), __float_as_uint(d));
                 if (P.ray_steps) P.ray_steps[tr.out_idx] = tr.steps;
                 if (P.ray_status) P.ray_status[tr.out_idx] = (uint8_t)st;
-                if (P.ray_drift) P.ray_drift[tr.out_idx] = (float)tr.drift;
+                if (P.ray_drift) P.ray_drift[tr.out_idx] = d;
                 alive = false;
             }
         }
     }
 
-    // launch totals: warp reduction, one atomic per warp and counter
-    for (int o = 16; o > 0; o >>= 1) {
-        cnt.steps += __shfl_down_sync(kFull, cnt.steps, o);
-        cnt.brick += __shfl_down_sync(kFull, cnt.brick, o);
-        cnt.rays += __shfl_down_sync(kFull, cnt.rays, o);
-#pragma unroll
-        for (int k = 0; k < 5; ++k) cnt.status[k] += __shfl_down_sync(kFull, cnt.status[k], o);
-        cnt.max_drift = fmaxf(cnt.max_drift, __shfl_down_sync(kFull, cnt.max_drift, o));
-        cnt.max_drift_escaped = fmaxf(cnt.max_drift_escaped, __shfl_down_sync(kFull, cnt.max_drift_escaped, o));
-    }
-    if (lane == 0 && P.stats) {
-        atomicAdd(&P.stats->ray_steps, cnt.steps);
-        atomicAdd(&P.stats->brick_steps, cnt.brick);
-        atomicAdd(&P.stats->rays, (unsigned long long)cnt.rays);
+    // block totals -> launch totals (non-negative floats order like their bit patterns)
+    __syncthreads();
+    if (threadIdx.x == 0 && P.stats) {
+        atomicAdd(&P.stats->ray_steps, bc->steps);
+        atomicAdd(&P.stats->brick_steps, bc->brick);
+        atomicAdd(&P.stats->rays, (unsigned long long)bc->rays);
         for (int k = 0; k < 5; ++k)
-            if (cnt.status[k]) atomicAdd(&P.stats->status[k], (unsigned long long)cnt.status[k]);
-        atomicAdd(&P.stats->queue_fetches, fetches);
-        // non-negative floats order like their bit patterns
-        atomicMax(reinterpret_cast<unsigned int *>(&P.stats->max_h_drift), __float_as_uint(cnt.max_drift));
+            if (bc->status[k]) atomicAdd(&P.stats->status[k], (unsigned long long)bc->status[k]);
+        atomicAdd(&P.stats->queue_fetches, bc->fetches);
+        atomicMax(reinterpret_cast<unsigned int *>(&P.stats->max_h_drift), __float_as_uint(bc->max_drift));
         atomicMax(reinterpret_cast<unsigned int *>(&P.stats->max_h_drift_escaped),
-                  __float_as_uint(cnt.max_drift_escaped));
+                  __float_as_uint(bc->max_drift_escaped));
     }
 }
 
@@ -795,6 +928,8 @@ static int check_config(const bhn_render_config *cfg) {
         return fail(BHN_ERR_VALUE, "tile_w * tile_h must be in [1, 4096]");
     if (cfg->refill_min < 1 || cfg->refill_min > 32) return fail(BHN_ERR_VALUE, "refill_min must be in [1, 32]");
     if (cfg->precision != 0 && cfg->precision != 1) return fail(BHN_ERR_VALUE, "precision must be 0 (fp32) or 1 (fp64)");
+    if (cfg->reg_cap != 0 && cfg->reg_cap != 80 && cfg->reg_cap != 64)
+        return fail(BHN_ERR_VALUE, "reg_cap must be 0, 80 or 64");
     return BHN_OK;
 }
 
@@ -812,8 +947,9 @@ static int launch_render(const void *records, const void *tables, int32_t nr, in
         reinterpret_cast<uintptr_t>(scratch) % 256 || reinterpret_cast<uintptr_t>(out) % 16)
         return fail(BHN_ERR_VALUE, "records/tables/out must be 16-byte and scratch 256-byte aligned");
     const int tables_bytes = (int)table_layout(nr, nt, np).total;
-    const int smem = tables_bytes + 8 * (n_views + 1);
-    if (smem > 200 * 1024) return fail(BHN_ERR_VALUE, "brick grids plus views exceed the shared-memory table budget");
+    const int64_t smem64 = smem_bytes(tables_bytes, n_views);
+    if (smem64 > 200 * 1024) return fail(BHN_ERR_VALUE, "brick grids plus views exceed the shared-memory table budget");
+    const int smem = (int)smem64;
     char *sc = static_cast<char *>(scratch);
     RenderParams P;
     P.records = records;
@@ -839,17 +975,17 @@ static int launch_render(const void *records, const void *tables, int32_t nr, in
     const dim3 grid((unsigned)(sms * cfg->blocks_per_sm)), block((unsigned)cfg->block_threads);
     BHN_CUDA_TRY(cudaMemsetAsync(&P.q->next, 0, sizeof(unsigned long long), s));
     BHN_CUDA_TRY(cudaMemsetAsync(P.stats, 0, sizeof(bhn_render_stats), s));
-    if (cfg->precision == 0) {
+    auto go = [&](auto kernel) -> int {
         if (smem > 48 * 1024)
-            BHN_CUDA_TRY(cudaFuncSetAttribute(render_kernel<Tracer32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        render_kernel<Tracer32><<<grid, block, smem, s>>>(P);
-    } else {
-        if (smem > 48 * 1024)
-            BHN_CUDA_TRY(cudaFuncSetAttribute(render_kernel<Tracer64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        render_kernel<Tracer64><<<grid, block, smem, s>>>(P);
-    }
-    BHN_LAUNCH_CHECK("render_kernel");
-    return BHN_OK;
+            BHN_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kernel<<<grid, block, smem, s>>>(P);
+        BHN_LAUNCH_CHECK("render_kernel");
+        return BHN_OK;
+    };
+    if (cfg->precision == 1) return go(render_kernel<Tracer64, 1>);
+    if (cfg->reg_cap == 64) return go(render_kernel<Tracer32, 4>);
+    if (cfg->reg_cap == 80) return go(render_kernel<Tracer32, 3>);
+    return go(render_kernel<Tracer32, 1>);
 }
 
 }  // namespace bhn

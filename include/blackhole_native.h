@@ -142,9 +142,18 @@ typedef struct bhn_view {
     int32_t width, height;
     int32_t x0, y0, crop_w, crop_h;
     int32_t max_steps;
-    int32_t pad0;
+    int32_t flags;           /* BHN_VIEW_* bits */
     int64_t out_offset;
 } bhn_view;
+
+/* Horizon guard (no reference counterpart; off = the reference's semantics):
+ * a ray moving inward (p_r < 0) from inside both the innermost photon orbit
+ * (the prograde equatorial circular photon orbit, inside which no ray from the
+ * camera can turn around) and the brick's inner radius is captured at that
+ * step.  In exact arithmetic no further emission can be added, so the image is
+ * unchanged; numerically it stops the h = 0.02 r RK2 step from overshooting
+ * into the horizon region, where it can fling a ray back through the brick. */
+#define BHN_VIEW_HORIZON_GUARD 1
 
 /* Launch shape, chosen by the autotuner. */
 typedef struct bhn_render_config {
@@ -153,6 +162,7 @@ typedef struct bhn_render_config {
     int32_t tile_w, tile_h;  /* ray order: rays of one tile are consecutive in the queue */
     int32_t refill_min;      /* a warp refills its dead lanes once this many (1..32) are dead */
     int32_t precision;       /* 0 = FP32 fused kernel, 1 = FP64 (oracle-matched) kernel */
+    int32_t reg_cap;         /* FP32 kernel register budget: 0 (compiler's choice), 80 or 64 */
 } bhn_render_config;
 
 /* Launch totals accumulated on the device (all zeroed by each launch). */

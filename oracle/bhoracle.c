@@ -386,7 +386,16 @@ void bho_trace_pixel(const bho_view *v, const double *coeffs, const double *rg, 
     int transfer_done = 0;
     int status = BHO_STATUS_MAX_STEPS;
     int32_t steps = 0, in_brick = 0;
+    /* Optional horizon guard (not part of the reference): an inbound ray inside
+     * both the innermost spherical photon orbit (prograde equatorial circular
+     * orbit, r = 2(1 + cos(2/3 acos(-|a|)))) and the brick's inner radius can
+     * add no more emission in exact arithmetic, so it is captured there. */
+    const double r_guard = (v->flags & 1) ? fmin(2.0 * (1.0 + cos((2.0 / 3.0) * acos(-fabs(a)))), rg[0]) : 0.0;
     for (int i = 1; i <= v->max_steps; ++i) {
+        if (y[1] < r_guard && y[4] < 0.0) {
+            status = BHO_STATUS_CAPTURED;
+            break;
+        }
         double h = v->h_scale * y[1];
         if (h < v->h_min) h = v->h_min;
         if (h > v->h_max) h = v->h_max;

@@ -86,7 +86,7 @@ typedef struct bho_view {
     int32_t width, height;                /* full image (NDC) */
     int32_t x0, y0, crop_w, crop_h;       /* rendered rectangle */
     int32_t max_steps;
-    int32_t pad;
+    int32_t flags;                        /* bit 0: horizon guard (not in the reference; see bhoracle.c) */
 } bho_view;
 
 enum { BHO_STATUS_MAX_STEPS = 0, BHO_STATUS_CAPTURED = 1, BHO_STATUS_ESCAPED = 2, BHO_STATUS_INVALID = 3 };

@@ -47,7 +47,7 @@ class View(ctypes.Structure):
         ("crop_w", ctypes.c_int32),
         ("crop_h", ctypes.c_int32),
         ("max_steps", ctypes.c_int32),
-        ("pad", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
     ]
 
 

@@ -20,7 +20,7 @@ def golden_view(g, name: str):
 
 def oracle_view(*, width, height, r_obs=1000.0, inclination_deg=17.0, phi_deg=0.0, fov_y_deg=None, roll_deg=0.0,
                 spin_a=0.9375, max_steps=4096, h_scale=0.02, h_min=1e-3, h_max=1.0, escape_radius=220.0,
-                affine_to_length_cm=1.0, max_optical_depth=30.0, crop=None):
+                affine_to_length_cm=1.0, max_optical_depth=30.0, crop=None, horizon_guard=False):
     if fov_y_deg is None:
         fov_y_deg = 2.0 * math.degrees(math.atan(20.0 / 1000.0))
     x0, y0, cw, ch = crop if crop is not None else (0, 0, width, height)
@@ -28,7 +28,8 @@ def oracle_view(*, width, height, r_obs=1000.0, inclination_deg=17.0, phi_deg=0.
                        phi_obs=math.radians(phi_deg), fov_y_deg=fov_y_deg, roll_deg=roll_deg, h_scale=h_scale,
                        h_min=h_min, h_max=h_max, escape_radius=escape_radius,
                        affine_to_length_cm=affine_to_length_cm, max_optical_depth=max_optical_depth, width=width,
-                       height=height, x0=x0, y0=y0, crop_w=cw, crop_h=ch, max_steps=max_steps)
+                       height=height, x0=x0, y0=y0, crop_w=cw, crop_h=ch, max_steps=max_steps,
+                       flags=1 if horizon_guard else 0)
 
 
 def view_to_oracle(v):
@@ -37,7 +38,7 @@ def view_to_oracle(v):
                        phi_deg=v.phi_deg, fov_y_deg=v.fov_y_deg, roll_deg=v.roll_deg, spin_a=v.spin_a,
                        max_steps=v.max_steps, h_scale=v.h_scale, h_min=v.h_min, h_max=v.h_max,
                        escape_radius=v.escape_radius, affine_to_length_cm=v.affine_to_length_cm,
-                       max_optical_depth=v.max_optical_depth, crop=v.rect)
+                       max_optical_depth=v.max_optical_depth, crop=v.rect, horizon_guard=v.horizon_guard)
 
 
 def linear_coeff_fixture(nphi: int = 2):
