@@ -799,7 +799,7 @@ __host__ __device__ inline int64_t smem_bytes(int tables_bytes, int n_views) {
 // ------------------------------------------------------------ persistent loop
 // MINB = resident 256-thread blocks the register allocation must allow:
 // 1 -> unconstrained, 3 -> <= 85 registers, 4 -> <= 64 registers.
-template <class Tracer, int MINB>
+template <class Tracer, int MINB, bool BATCH>
 __global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     int64_t *vbegin = reinterpret_cast<int64_t *>(smem + align16(P.tables_bytes));
@@ -844,9 +844,59 @@ __global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P)
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     Tracer tr;
-    bool alive = false, exhausted = false;
+    bool alive = false, exhausted = BATCH;
 
-    while (true) {
+    // Batch mode (refill_min = 32): a warp takes 32 consecutive ray slots with one
+    // atomic and every lane traces its ray to the end in a tight loop; the warp
+    // fetches again once all 32 are done.  No per-step warp vote.
+    while (BATCH) {
+        unsigned long long base = 0;
+        if (lane == 0) {
+            base = atomicAdd(&P.q->next, 32ull);
+            atomicAdd(&bc->fetches, 1ull);
+        }
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= total) break;
+        const unsigned long long slot = base + lane;
+        if (slot < total) {
+            const int vi = P.n_views == 1 ? 0 : find_view(vbegin, P.n_views, (int64_t)slot);
+            const ViewDev &v = P.views[vi];
+            const PixelRef px = pixel_of(v, (int64_t)slot - vbegin[vi], P.tile_w, P.tile_h);
+            if (v.valid && v.max_steps > 0) {
+                tr.init(v, vi, px.px, px.py, px.out_idx);
+                const StepConst &C = sconst[vi];
+                int st;
+                do {
+                    st = tr.step(C, T, rec, P.nr, P.nt, P.np, P.views);
+                } while (st < 0);
+                tr.finish(P.out, st, C, P.views);
+                const float d = tr.drift_f();
+                atomicAdd(&bc->steps, (unsigned long long)tr.steps);
+                atomicAdd(&bc->brick, (unsigned long long)tr.brick);
+                atomicAdd(&bc->rays, 1u);
+                atomicAdd(&bc->status[st], 1u);
+                atomicMax(reinterpret_cast<unsigned int *>(&bc->max_drift), __float_as_uint(d));
+                if (st == BHN_RAY_ESCAPED)
+                    atomicMax(reinterpret_cast<unsigned int *>(&bc->max_drift_escaped), __float_as_uint(d));
+                if (P.ray_steps) P.ray_steps[tr.out_idx] = tr.steps;
+                if (P.ray_status) P.ray_status[tr.out_idx] = (uint8_t)st;
+                if (P.ray_drift) P.ray_drift[tr.out_idx] = d;
+            } else {
+                Tracer::write_zero(P.out, px.out_idx);
+                const int zst = v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID;
+                atomicAdd(&bc->rays, 1u);
+                atomicAdd(&bc->status[zst], 1u);
+                if (P.ray_steps) P.ray_steps[px.out_idx] = 0;
+                if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)zst;
+                if (P.ray_drift) P.ray_drift[px.out_idx] = 0.0f;
+            }
+        }
+        __syncwarp();
+    }
+
+    // Compaction mode (refill_min < 32): every step, the warp votes; once
+    // refill_min lanes are done it refills them with one atomic (ballot + popc).
+    while (!BATCH && (!exhausted || __any_sync(kFull, alive))) {
         const unsigned dead = __ballot_sync(kFull, !alive);
         const int ndead = __popc(dead);
         if (!exhausted && ndead > 0 && (ndead >= P.refill_min || ndead == 32)) {
@@ -982,10 +1032,11 @@ static int launch_render(const void *records, const void *tables, int32_t nr, in
         BHN_LAUNCH_CHECK("render_kernel");
         return BHN_OK;
     };
-    if (cfg->precision == 1) return go(render_kernel<Tracer64, 1>);
-    if (cfg->reg_cap == 64) return go(render_kernel<Tracer32, 4>);
-    if (cfg->reg_cap == 80) return go(render_kernel<Tracer32, 3>);
-    return go(render_kernel<Tracer32, 1>);
+    const bool batch = cfg->refill_min >= 32;
+    if (cfg->precision == 1) return batch ? go(render_kernel<Tracer64, 1, true>) : go(render_kernel<Tracer64, 1, false>);
+    if (cfg->reg_cap == 64) return batch ? go(render_kernel<Tracer32, 4, true>) : go(render_kernel<Tracer32, 4, false>);
+    if (cfg->reg_cap == 80) return batch ? go(render_kernel<Tracer32, 3, true>) : go(render_kernel<Tracer32, 3, false>);
+    return batch ? go(render_kernel<Tracer32, 1, true>) : go(render_kernel<Tracer32, 1, false>);
 }
 
 }  // namespace bhn

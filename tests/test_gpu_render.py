@@ -205,12 +205,29 @@ def test_full_config2_properties(c2_brick):
     assert st.ray_steps == int(full.per_ray("steps").to(torch.int64).sum())
     crop = bn.render(db, bn.View(1024, 1024, max_steps=4096, crop=(300, 700, 50, 30)), precision="fp32").image()
     assert torch.equal(img[700:730, 300:350], crop)
-    # FP32 against the FP64 kernel (itself checked against the oracle on crops), horizon guard on
+    # FP32 against the FP64 kernel (itself checked against the oracle on crops),
+    # horizon guard on, on the pixels where the FP64 method is well conditioned
     vg = bn.View(1024, 1024, max_steps=4096, horizon_guard=True)
     f64 = bn.render(db, vg, precision="fp64").image().cpu().numpy()
+    cond = conditioned_pixels(db, vg, f64)
+    assert cond.mean() >= 0.99
     i32 = bn.render(db, vg, precision="fp32").image().cpu().numpy().astype(np.float64)
-    assert rel_l1(i32[..., 0], f64[..., 0]) <= FP32_I_REL_L1
-    assert flux_weighted_dm(i32, f64) <= FP32_DM
+    assert rel_l1(i32[..., 0][cond], f64[..., 0][cond]) <= FP32_I_REL_L1
+    assert flux_weighted_dm(i32[cond], f64[cond]) <= FP32_DM
+
+
+def conditioned_pixels(db, view, f64_img):
+    """Pixels whose FP64 Stokes I is a well-conditioned function of the inputs:
+    finite, non-negative and moved by less than 1e-4 (relative) when every
+    step bound is scaled by 1 + 1e-6.  Rays that graze the spin axis (the
+    reference's clamped 1/sin^2 theta makes its coordinate ds explode there)
+    or overshoot into the horizon amplify rounding-level perturbations without
+    bound; no finite-precision result can be compared with another there."""
+    pert = bn.render(db, view.scaled_step(1.0 + 1e-6), precision="fp64").image().cpu().numpy()
+    I, Ip = f64_img[..., 0], pert[..., 0]
+    ok = np.isfinite(I) & np.isfinite(Ip) & (I >= 0.0)
+    scale = float(np.mean(np.abs(I[ok]))) if ok.any() else 1.0
+    return ok & (np.abs(I - Ip) <= 1e-4 * np.abs(I) + 1e-6 * scale)
 
 
 def test_zero_steps_and_no_brick_hits(golden_brick):
