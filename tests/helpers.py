@@ -71,9 +71,16 @@ def pol_fraction(img):
     return np.sqrt(img[..., 1] ** 2 + img[..., 2] ** 2) / I
 
 
-def flux_weighted_dm(a, b):
-    """Flux-weighted mean |m_a - m_b| over pixels with I_b > 0."""
-    w = np.maximum(b[..., 0], 0.0)
+def flux_weighted_dm(a, b, floor: float = 1e-6):
+    """Flux-weighted mean |m_a - m_b| (weights I_b) over the pixels that carry
+    flux: I_b and I_a above ``floor`` times the peak I_b (the polarization
+    fraction of a pixel with no intensity is undefined)."""
+    Ib = b[..., 0]
+    if not np.any(Ib > 0):
+        return 0.0
+    lit = (Ib > floor * Ib.max()) & (a[..., 0] > floor * Ib.max())
+    w = np.where(lit, Ib, 0.0)
     if w.sum() <= 0:
         return 0.0
-    return float(np.sum(w * np.abs(pol_fraction(a) - pol_fraction(b))) / np.sum(w))
+    dm = np.abs(pol_fraction(a) - pol_fraction(b))
+    return float(np.sum(w[lit] * dm[lit]) / np.sum(w[lit]))
