@@ -1,6 +1,6 @@
 """Build ``libbhnative.so`` (the sm_100a CUDA library behind ``blackhole_native``).
 
-    python -m blackhole_native._build        # from the blackhole-sim_b200 directory
+    python blackhole-sim_b200/blackhole_native/_build.py   # a plain script: it does not import the package
 
 The library is compiled in-tree next to this file so that it travels with the
 source tree; it links the CUDA runtime statically.
