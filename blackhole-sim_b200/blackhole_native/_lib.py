@@ -22,9 +22,10 @@ EXPORTED = (
     "bhn_stokes_rk2_brick", "bhn_sample_brick_trilinear", "bhn_sample_and_step_stokes",
     "bhn_sample_brick_valid_mask", "bhn_check_values",
     "bhn_brick_tables_bytes", "bhn_brick_build_tables", "bhn_brick_pack", "bhn_brick_locate",
-    "bhn_render_scratch_bytes", "bhn_render_prepare", "bhn_render_launch",
+    "bhn_render_scratch_bytes", "bhn_render_prepare", "bhn_render_launch", "bhn_render_noalloc",
     "bhn_graph_create", "bhn_graph_launch", "bhn_graph_destroy",
 )
+NOALLOC_MAX_VIEWS = 120  # BHN_NOALLOC_MAX_VIEWS
 
 
 class ViewStruct(ctypes.Structure):
@@ -121,13 +122,20 @@ def _declare(lib: ctypes.CDLL) -> None:
         "bhn_render_prepare": ([ctypes.POINTER(ViewStruct), i32, vp, i64, vp], ctypes.c_int),
         "bhn_render_launch": ([vp, vp, i32, i32, i32, i32, ctypes.POINTER(RenderConfigStruct), vp,
                                ctypes.POINTER(RayOutputsStruct), vp, i64, vp, vp], ctypes.c_int),
+        "bhn_render_noalloc": ([vp, vp, i32, i32, i32, ctypes.POINTER(ViewStruct), i32,
+                                ctypes.POINTER(RenderConfigStruct), vp, ctypes.POINTER(RayOutputsStruct), vp, vp],
+                               ctypes.c_int),
         "bhn_graph_create": ([vp, vp, i32, i32, i32, i32, ctypes.POINTER(RenderConfigStruct), vp,
                               ctypes.POINTER(RayOutputsStruct), vp, i64, vp, ctypes.POINTER(vp)], ctypes.c_int),
         "bhn_graph_launch": ([vp, vp], ctypes.c_int),
         "bhn_graph_destroy": ([vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
-        fn = getattr(lib, name)
+        try:
+            fn = getattr(lib, name)
+        except AttributeError as exc:
+            raise ImportError(f"blackhole_native: {LIB_PATH} lacks {name}; the library is older than its "
+                              "binding -- rebuild it with `python blackhole-sim_b200/blackhole_native/_build.py`") from exc
         fn.argtypes = args
         fn.restype = res
 
@@ -139,7 +147,7 @@ def lib() -> ctypes.CDLL:
         if not LIB_PATH.exists():
             raise ImportError(
                 f"blackhole_native: CUDA library {LIB_PATH} is missing; build it with "
-                "`python -m blackhole_native._build` (nvcc, sm_100a)")
+                "`python blackhole-sim_b200/blackhole_native/_build.py` (nvcc, sm_100a)")
         handle = ctypes.CDLL(str(LIB_PATH))
         _declare(handle)
         _lib = handle

@@ -205,6 +205,25 @@ int bhn_render_launch(const void *records, const void *tables, int32_t nr, int32
                       const bhn_render_config *cfg, void *out, const bhn_ray_outputs *ray_out, void *scratch,
                       int64_t scratch_bytes, bhn_render_stats *stats, void *stream);
 
+/* bhn_render_prepare + bhn_render_launch for callers that cannot allocate
+ * device memory (no counterpart in the reference).  Code that runs while a
+ * stream is being captured into a CUDA graph may not call cudaMalloc, and some
+ * hosts own all device memory through their own allocator; such callers pass
+ * only inputs and outputs.  The scratch is a fixed 64 KiB array in the
+ * library's device image (held by every GPU that loads the library until the
+ * process exits), so at most BHN_NOALLOC_MAX_VIEWS views fit in one call; more
+ * is rejected with BHN_ERR_VALUE.  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress) with the device current, so
+ * make the first call on each device before any stream capture.  All calls on
+ * a device share the array: calls that overlap on the GPU (different streams,
+ * or the same stream from several host threads without ordering) race.  The
+ * function allocates nothing (no cudaMalloc / cudaFree); h_views is host
+ * memory copied before return; stats may be NULL. */
+#define BHN_NOALLOC_MAX_VIEWS 120
+int bhn_render_noalloc(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np,
+                       const bhn_view *h_views, int32_t n_views, const bhn_render_config *cfg, void *out,
+                       const bhn_ray_outputs *ray_out, bhn_render_stats *stats, void *stream);
+
 /* CUDA-graph form of bhn_render_launch: captures the queue reset and the
  * persistent launch once; bhn_graph_launch replays it on `stream`. */
 typedef struct bhn_graph bhn_graph;
