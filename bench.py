@@ -392,6 +392,85 @@ def bench_ours(args) -> dict | None:
     return line if rank == 0 else None
 
 
+def bench_views(args) -> dict | None:
+    """Many uneven views (seeded: side 64..1024, a ~ U(0, 0.998), inclination
+    ~ U(5, 85) deg, max_steps ~ U{512..8192}) through one shared 128x64x128x11
+    float32 brick, all in one persistent CUDA-graph launch."""
+    import torch
+
+    import blackhole_native as bn
+    from blackhole_native import autotune, scenes
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    init_dist(world, "nccl")
+    db = bn.DeviceBrick(scenes.shared_brick(), device=device, precisions=("fp32",))
+    views = scenes.uneven_views(args.n_views, seed=0)
+    key = f"views{args.n_views}"
+    if args.tune:
+        space = dict(autotune.DEFAULT_SPACE, block_threads=(128, 256), blocks_per_sm=(2, 4))
+        best = autotune.tune(db, views[:48], key, space=space, repeats=2,
+                             log=lambda m: print(m, file=sys.stderr, flush=True))
+        print(json.dumps({"autotune": key, "best": best.__dict__, "cache": str(autotune.CACHE)}), flush=True)
+        return None
+    cfg = bn.RenderConfig(**args.config) if args.config else (autotune.cached_config(key, device) or bn.RenderConfig())
+    rnd = bn.Renderer(db, views, config=cfg, precision="fp32")
+    stream = torch.cuda.current_stream(device)
+    rnd.capture()
+    for _ in range(args.warmup):
+        rnd.graph_launch()
+    torch.cuda.synchronize(device)
+    st = rnd.result().stats()
+    K = args.steps
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    barrier(world)
+    torch.cuda.synchronize(device)
+    evs[0].record(stream)
+    for i in range(K):
+        rnd.graph_launch()
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    total_ms = evs[0].elapsed_time(evs[K])
+    t_max = max_over_ranks(total_ms, world, device)
+    value = sum_over_ranks(st.ray_steps * K, world, device) / (t_max * 1e-3)
+    rnd.release_graph()
+    # per view, each rendered alone (same launch shape)
+    per_view = []
+    for v in views:
+        r1 = bn.Renderer(db, [v], config=cfg, precision="fp32")
+        r1.launch()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r1.launch()
+        b.record(stream)
+        b.synchronize()
+        s1 = r1.result().stats()
+        per_view.append(s1.ray_steps / (a.elapsed_time(b) * 1e-3))
+    pv = np.asarray(per_view)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"batched persistent launch: {len(views)} seeded views (side 64-1024, a~U(0,0.998), "
+                               "incl~U(5,85)deg, max_steps~U{512..8192}), shared 128x64x128x11 float32 brick, "
+                               "one CUDA-graph launch",
+                   "rays_per_step": st.rays, "ray_steps_per_step": st.ray_steps,
+                   "autotune": {"block_threads": cfg.block_threads, "blocks_per_sm": cfg.blocks_per_sm,
+                                "tile": [cfg.tile_w, cfg.tile_h], "refill_min": cfg.refill_min,
+                                "reg_cap": cfg.reg_cap}},
+        "per_view_ray_steps_per_s": {"min": float(pv.min()), "median": float(np.median(pv)),
+                                     "max": float(pv.max()), "views": len(pv)},
+        "status_counts": st.status, "gpu_launches": K,
+    }
+    if world > 1:
+        import torch.distributed as td
+
+        td.destroy_process_group()
+    return line if rank == 0 else None
+
+
 def bench_reference(args) -> dict | None:
     rank, world, _ = dist_env()
     if rank != 0:
@@ -436,11 +515,19 @@ def main(argv=None) -> int:
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")
     ap.add_argument("--tune", action="store_true", help="run the launch-shape autotuner on the workload and exit")
+    ap.add_argument("--workload", choices=["image", "views"], default="image",
+                    help="image: the 1024x1024 single view (default); views: many uneven views in one launch")
+    ap.add_argument("--n-views", type=int, default=256)
     ap.add_argument("--side", type=int, default=0,
                     help="render side x side rays of the same scene instead of 1024x1024 (profiling only)")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, whatever is asked
-    line = bench_reference(args) if args.impl == "reference" else bench_ours(args)
+    if args.impl == "reference":
+        line = bench_reference(args)
+    elif args.workload == "views":
+        line = bench_views(args)
+    else:
+        line = bench_ours(args)
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0
