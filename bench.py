@@ -51,7 +51,7 @@ BYTES_PER_BRICK_STEP = 8 * 11 * 4     # 8 corners x 11 float32 channels
 BYTES_PER_RAY = 16                    # float4 Stokes written once per ray
 MEASURED_PEAKS = REPO / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
-PROFILE_SUMMARY = REPO / "profiles" / "render_kernel_fp32_config2.md"
+PROFILE_SUMMARY = REPO / "profiles" / "render_kernel_fp32_image1024.md"
 
 
 # ------------------------------------------------------------------ helpers
@@ -255,14 +255,14 @@ def bench_ours(args) -> dict | None:
     if args.tune:
         from blackhole_native import autotune
 
-        best = autotune.tune(db, [view], "config2", log=lambda m: print(m, file=sys.stderr, flush=True))
-        print(json.dumps({"autotune": "config2", "best": best.__dict__, "cache": str(autotune.CACHE)}), flush=True)
+        best = autotune.tune(db, [view], "image1024", log=lambda m: print(m, file=sys.stderr, flush=True))
+        print(json.dumps({"autotune": "image1024", "best": best.__dict__, "cache": str(autotune.CACHE)}), flush=True)
         return None
     cfg = bn.RenderConfig(**args.config) if args.config else None
     if cfg is None:
         from blackhole_native import autotune
 
-        cfg = autotune.cached_config("config2", device) or bn.RenderConfig()
+        cfg = autotune.cached_config("image1024", device) or bn.RenderConfig()
     rnd = bn.Renderer(db, [view], config=cfg, precision="fp32")
     stream = torch.cuda.current_stream(device)
 

@@ -22,6 +22,7 @@
 //   Tracer64 -- FP64 throughout with the reference's own formulation of the
 //               right-hand side; the GPU form of the CPU oracle, used for the
 //               fine-step precision study on images too large for the CPU.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -1138,3 +1139,4 @@ int bhn_graph_destroy(bhn_graph *graph) {
 }
 
 }  // extern "C"
+#include "bhn_learned.cuh"

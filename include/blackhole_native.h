@@ -224,6 +224,61 @@ int bhn_render_noalloc(const void *records, const void *tables, int32_t nr, int3
                        const bhn_view *h_views, int32_t n_views, const bhn_render_config *cfg, void *out,
                        const bhn_ray_outputs *ray_out, bhn_render_stats *stats, void *stream);
 
+/* ---- learned step-size proposal (no reference counterpart) ----
+ * The plain method is kerr.py:337-384's loop with the RK2 step of
+ * native/cuda/kerr_stokes_kernel.cu:13 at h = clamp(h_scale r, h_min, h_max).
+ * These entry points add (1) an RK2 step-doubling controller that renders the
+ * adaptive image and records training samples, (2) training kernels for an
+ * 8 -> 64 -> 64 -> 1 SiLU network (BF16 weights, FP32 accumulation) that maps
+ * the ray state to log h, and (3) the ray loop that takes the network's step
+ * and falls back to the plain step when an embedded error check fails.  All
+ * three always apply BHN_VIEW_HORIZON_GUARD. */
+typedef struct bhn_adapt_params {
+    float tol;           /* mixed-norm tolerance: |e_i| <= tol (1 + |y_i|) over r, theta, phi, p_r, p_theta */
+    float sample_prob;   /* controller: probability of recording an accepted step */
+    float h_floor, h_ceil;
+    float margin;        /* learned: subtracted from the proposed log h */
+    float check_tol;     /* learned: tolerance of the embedded Euler-midpoint check h|k2 - k1| (0: none) */
+    int32_t interval;    /* learned: steps between network evaluations (the proposal scales with r between) */
+    int32_t max_attempts;
+    uint32_t seed;
+} bhn_adapt_params;
+
+/* Sample rows: 8 raw features (log r, cos theta, p_r, p_theta, a, log|Delta|,
+ * p_phi, log(j_I + 1e-12)) followed by log h_opt, h_opt = h err^(-1/3) the step
+ * at which the controller's error estimate equals the tolerance (9 floats). */
+#define BHN_SAMPLE_FLOATS 9
+int64_t bhn_mlp_param_count(void);
+int64_t bhn_mlp_blob_bytes(void);
+/* FP32 parameters [W1 8x64 | b1 | W2 64x64 | b2 | W3 64 | b3] (device) +
+ * h_norm (host: mu_x[8], 1/sigma_x[8], mu_y, sigma_y) -> inference blob (BF16
+ * fragments, device). */
+int bhn_mlp_pack(const float *params, const float *h_norm, void *blob, void *stream);
+/* grad += d(mean squared error)/d(params) over rows index[first .. first+count)
+ * of standardised samples; loss += sum of squared errors. */
+int bhn_mlp_grad(const float *params, const float *samples, const int64_t *index, int64_t first, int64_t count,
+                 float *grad, float *loss, void *stream);
+/* One Adam step (step counts from 1); clears grad. */
+int bhn_mlp_adam(float *params, float *grad, float *m, float *v, float lr, float beta1, float beta2, float eps,
+                 int32_t step, void *stream);
+/* The inference path on given standardised feature rows (n x 8) -> n outputs. */
+int bhn_mlp_infer(const void *blob, const float *features, int64_t n, float *out, void *stream);
+/* Step-doubling controller over prepared views (bhn_render_prepare): float4
+ * Stokes out, optional per-ray steps/status, samples appended while
+ * *sample_count < capacity; counters[0..2] += RK2 stage pairs, accepted steps,
+ * rejected attempts. */
+int bhn_adaptive_launch(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np, int32_t n_views,
+                        const bhn_render_config *cfg, void *out, const bhn_ray_outputs *ray_out, void *scratch,
+                        int64_t scratch_bytes, const bhn_adapt_params *params, float *samples,
+                        unsigned long long *sample_count, unsigned long long sample_capacity,
+                        unsigned long long *counters, void *stream);
+/* The learned-step ray loop over prepared views; counters[0..3] += RHS
+ * evaluations, steps, fallbacks to the plain step, network evaluations. */
+int bhn_learned_launch(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np, int32_t n_views,
+                       const bhn_render_config *cfg, void *out, const bhn_ray_outputs *ray_out, void *scratch,
+                       int64_t scratch_bytes, const bhn_adapt_params *params, const void *blob,
+                       unsigned long long *counters, void *stream);
+
 /* CUDA-graph form of bhn_render_launch: captures the queue reset and the
  * persistent launch once; bhn_graph_launch replays it on `stream`. */
 typedef struct bhn_graph bhn_graph;

@@ -37,7 +37,7 @@ def golden_brick(ray_golden):
 
 
 @pytest.fixture(scope="module")
-def c2_brick():
+def scene_brick():
     b = bricks.torus_brick(256, 128, 256, spin_a=0.9375, seed=0, dtype=np.float32)
     return b, bn.DeviceBrick(b, precisions=("fp32", "fp64"))
 
@@ -77,7 +77,7 @@ def test_fp32_kernel_within_tolerance(ray_golden, golden_brick, name):
     assert flux_weighted_dm(img, ref) <= FP32_DM
 
 
-def test_c2_crop_parity(c2_brick):
+def test_scene_crop_parity(scene_brick):
     """1024x1024 camera, 4096 steps, 256x128x256 float32 torus brick: the
     central 64x64 crop against the oracle.
 
@@ -87,7 +87,7 @@ def test_c2_crop_parity(c2_brick):
     kernel is held to the FP32 bar on the pixels the horizon guard leaves
     unchanged (where the method is well conditioned), and on every pixel
     with the guard on."""
-    b, db = c2_brick
+    b, db = scene_brick
     v = bn.View(1024, 1024, max_steps=4096, crop=(480, 480, 64, 64))
     o_img, o_steps, o_status, _ = _oracle(v, b)
     r64 = bn.render(db, v, precision="fp64", ray_outputs=True)
@@ -109,8 +109,8 @@ def test_c2_crop_parity(c2_brick):
     assert rel_l1(g64, g_img) <= 1e-7
 
 
-def test_horizon_guard_only_touches_captured_rays(c2_brick):
-    b, db = c2_brick
+def test_horizon_guard_only_touches_captured_rays(scene_brick):
+    b, db = scene_brick
     v = bn.View(1024, 1024, max_steps=4096, crop=(400, 440, 96, 64))
     off = bn.render(db, v, precision="fp64", ray_outputs=True)
     on = bn.render(db, bn.View(1024, 1024, max_steps=4096, crop=(400, 440, 96, 64), horizon_guard=True),
@@ -121,8 +121,8 @@ def test_horizon_guard_only_touches_captured_rays(c2_brick):
     assert np.all(on.per_ray("steps").cpu().numpy()[cap] <= off.per_ray("steps").cpu().numpy()[cap])
 
 
-def test_locate_bit_exact(c2_brick):
-    b, db = c2_brick
+def test_locate_bit_exact(scene_brick):
+    b, db = scene_brick
     rng = np.random.default_rng(11)
     n = 200_000
     pts = np.stack([rng.uniform(b.r[0], b.r[-1], n), rng.uniform(b.theta[0], b.theta[-1], n),
@@ -146,9 +146,9 @@ def test_locate_bit_exact(c2_brick):
     assert out[:, 3].tolist() == [0, 0]
 
 
-def test_batched_views_equal_single_views(c2_brick):
+def test_batched_views_equal_single_views(scene_brick):
     """Uneven views in one persistent launch give the same pixels as separate launches."""
-    b, db = c2_brick
+    b, db = scene_brick
     views = [bn.View(48, 40, inclination_deg=30.0, max_steps=2000),
              bn.View(1024, 1024, crop=(500, 500, 24, 17), max_steps=4096),
              bn.View(16, 16, spin_a=0.3, inclination_deg=80.0, r_obs=60.0, fov_y_deg=30.0, max_steps=700)]
@@ -166,16 +166,16 @@ def test_batched_views_equal_single_views(c2_brick):
 
 @pytest.mark.parametrize("cfg", [bn.RenderConfig(64, 8, 1, 1, 32), bn.RenderConfig(256, 2, 16, 2, 8),
                                  bn.RenderConfig(128, 4, 4, 8, 1)])
-def test_launch_shape_does_not_change_pixels(c2_brick, cfg):
-    b, db = c2_brick
+def test_launch_shape_does_not_change_pixels(scene_brick, cfg):
+    b, db = scene_brick
     v = bn.View(1024, 1024, crop=(448, 448, 128, 96))
     ref = bn.render(db, v, precision="fp32").image()
     got = bn.render(db, v, precision="fp32", config=cfg).image()
     assert torch.equal(ref, got)
 
 
-def test_graph_replay_equals_launch(c2_brick):
-    b, db = c2_brick
+def test_graph_replay_equals_launch(scene_brick):
+    b, db = scene_brick
     v = bn.View(1024, 1024, crop=(400, 400, 200, 200))
     r = bn.Renderer(db, [v], precision="fp32")
     a = r.launch().image().clone()
@@ -191,11 +191,11 @@ def test_graph_replay_equals_launch(c2_brick):
     r.release_graph()
 
 
-def test_full_config2_properties(c2_brick):
+def test_full_image1024_properties(scene_brick):
     """Full 1024x1024, 4096-step image: size-independent properties -- a crop of
     the full image equals the crop rendered alone, the FP32 image is within
     tolerance of the FP64 kernel, every pixel is finite and accounted for."""
-    b, db = c2_brick
+    b, db = scene_brick
     v = bn.View(1024, 1024, max_steps=4096)
     full = bn.render(db, v, precision="fp32", ray_outputs=True)
     img = full.image()
