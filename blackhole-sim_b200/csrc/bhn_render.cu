@@ -234,6 +234,14 @@ __device__ __forceinline__ void split(double v, float &hi, float &lo) {
 }
 
 constexpr double kNearHorizon = 0.1;  // FP64 island: steps that start within 0.1 M of r+
+// FP64 island next to the spin axis and at extreme momenta.  A ray that
+// grazes the axis meets the clamped sin(theta) = 1e-7 (kerr.py:93), where
+// p_theta' ~ p_phi^2 cos / sin^3 throws p_theta to ~1e21; the FP64 method
+// carries such a ray on (its squares ~1e42 stay finite), FP32's would overflow
+// and end the ray as invalid.  Steps that start within 1e-4 rad of a pole or
+// with |p_r| or |p_theta| >= 1e15 therefore run in FP64.
+constexpr float kPoleIsland = 1.0e-4f;
+constexpr float kMomentumIsland = 1.0e15f;
 
 // ------------------------------------------------------------ FP64 helpers
 // kerr.py:52-64, :86-102, :236-303 in FP64 (the oracle's formulation).
@@ -455,7 +463,9 @@ struct Tracer32 {
 
     // The FP64 island next to the horizon: the whole RK2 step in FP64, since
     // p_r ~ 1/Delta leaves FP32's exponent range there.
-    __device__ __forceinline__ bool step_fp64(const ViewDev &v, float &dr, float &dph) {
+    // Returns 0 (finite), 1 (non-finite) or 2 (horizon guard: the midpoint lies
+    // inside the horizon; the state is left unchanged).
+    __device__ __forceinline__ int step_fp64(const ViewDev &v, bool guard, float &dr, float &dph) {
         const double r = (double)rh + (double)rl;
         const double th = (double)th_h + (double)th_l;
         const double ph = (double)ph_h + (double)ph_l;
@@ -464,6 +474,7 @@ struct Tracer32 {
         rhs64h(r, th, pr, pth, pt, pphi, v.a, v.r_plus, v.r_minus, k1);
         drift = fmaxf(drift, (float)fabs(fabs(k1.H) - (double)H0));
         const double hh = 0.5 * h;
+        if (guard && r + hh * k1.r < v.r_plus) return 2;
         rhs64h(r + hh * k1.r, th + hh * k1.th, pr + hh * k1.pr, pth + hh * k1.pth, pt, pphi, v.a, v.r_plus,
                v.r_minus, k2);
         const double rn = r + h * k2.r, thn = safe_theta(th + h * k2.th), phn = ph + h * k2.ph;
@@ -475,7 +486,7 @@ struct Tracer32 {
         split(phn, ph_h, ph_l);
         pr = (float)prn;
         pth = (float)pthn;
-        return isfinite(rn) && isfinite(thn) && isfinite(phn) && isfinite(prn) && isfinite(pthn);
+        return (isfinite(rn) && isfinite(thn) && isfinite(phn) && isfinite(prn) && isfinite(pthn)) ? 0 : 1;
     }
 
     // One RK2 geodesic step plus its brick segment.  Returns -1 while the ray
@@ -486,11 +497,13 @@ struct Tracer32 {
         const float r0 = rh + rl, th0 = th_h + th_l, ph0 = ph_h + ph_l;
         float dr, dph;
         bool finite;
-        if (rh < C.r_near) {
-            finite = step_fp64(views[vi], dr, dph);
+        const bool south = th_h > kHalfPiF;
+        const float d0 = south ? (kPiH - th_h) + (kPiL - th_l) : th0;
+        if (rh < C.r_near || d0 < kPoleIsland || !(fabsf(pth) < kMomentumIsland && fabsf(pr) < kMomentumIsland)) {
+            const int rc = step_fp64(views[vi], C.r_guard > 0.0f, dr, dph);
+            if (rc == 2) return BHN_RAY_CAPTURED;
+            finite = rc == 0;
         } else {
-            const bool south = th_h > kHalfPiF;
-            const float d0 = south ? (kPiH - th_h) + (kPiL - th_l) : th0;
             float s, c;
             sincos_pole(d0, south, s, c);
             const float x0 = (rh - C.rp_h) + (rl - C.rp_l);
@@ -499,6 +512,8 @@ struct Tracer32 {
             rhs32(r0, x0, s, c, pr, pth, pt, pphi, C.a, C.a2, C.dpm, k1);
             drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
             const float hh = 0.5f * h;
+            // horizon guard: a step whose midpoint lies inside the horizon is not taken
+            if (C.r_guard > 0.0f && fmaf(hh, k1.r, x0) < 0.0f) return BHN_RAY_CAPTURED;
             // midpoint: pole distance clamped at eps like kerr.py:35-36 inside the right-hand side
             const float dm = fmaxf(south ? fmaf(-hh, k1.th, d0) : fmaf(hh, k1.th, d0), kEpsF);
             sincos_pole(dm, south, s, c);
@@ -680,6 +695,8 @@ struct Tracer64 {
         rhs64(r, th, pr, pth, pt, pphi, v.a, k1);
         drift = fmax(drift, fabs(fabs(k1.H) - H0));
         const double hh = 0.5 * h;
+        // horizon guard: a step whose midpoint lies inside the horizon is not taken
+        if (C.r_guard > 0.0f && r + hh * k1.r < v.r_plus) return BHN_RAY_CAPTURED;
         rhs64(r + hh * k1.r, th + hh * k1.th, pr + hh * k1.pr, pth + hh * k1.pth, pt, pphi, v.a, k2);
         const double rn = r + h * k2.r;
         const double thn = safe_theta(th + h * k2.th);

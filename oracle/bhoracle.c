@@ -389,7 +389,11 @@ void bho_trace_pixel(const bho_view *v, const double *coeffs, const double *rg, 
     /* Optional horizon guard (not part of the reference): an inbound ray inside
      * both the innermost spherical photon orbit (prograde equatorial circular
      * orbit, r = 2(1 + cos(2/3 acos(-|a|)))) and the brick's inner radius can
-     * add no more emission in exact arithmetic, so it is captured there. */
+     * add no more emission in exact arithmetic, so it is captured there.  A
+     * step whose RK2 midpoint (the Euler half step) lies inside the horizon is
+     * not taken either: its second stage would be evaluated where Delta < 0,
+     * which flings the ray back out with garbage momenta; the ray is captured
+     * at that step's start. */
     const double r_guard = (v->flags & 1) ? fmin(2.0 * (1.0 + cos((2.0 / 3.0) * acos(-fabs(a)))), rg[0]) : 0.0;
     for (int i = 1; i <= v->max_steps; ++i) {
         if (y[1] < r_guard && y[4] < 0.0) {
@@ -399,6 +403,14 @@ void bho_trace_pixel(const bho_view *v, const double *coeffs, const double *rg, 
         double h = v->h_scale * y[1];
         if (h < v->h_min) h = v->h_min;
         if (h > v->h_max) h = v->h_max;
+        if (r_guard > 0.0) {
+            double k1[6];
+            bho_geodesic_rhs(y, a, pt, pphi, k1);
+            if (y[1] + 0.5 * h * k1[1] < r_plus) {
+                status = BHO_STATUS_CAPTURED;
+                break;
+            }
+        }
         double yn[6];
         bho_rk2_step(y, h, a, pt, pphi, yn);
         steps++;
