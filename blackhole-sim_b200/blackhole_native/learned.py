@@ -4,16 +4,22 @@ Pipeline (all compute in this package's CUDA kernels):
 
 1. ``generate_samples`` runs the step-doubling RK2 controller over seeded
    scenes; every accepted step may be recorded as (8 features at the step
-   start, log h_opt), h_opt = h err^(-1/3) the step whose estimated RK2 error
-   equals the tolerance -- a function of the local state only.
+   start, log(h_opt / h_plain)): h_opt = h err^(-1/3) is the step whose
+   estimated RK2 error equals the tolerance -- a function of the local state
+   only -- and h_plain = clamp(h_scale r, h_min, h_max) the plain step there.
 2. ``train`` fits the 8 -> 64 -> 64 -> 1 SiLU network (BF16 weights, FP32
-   accumulation) to standardised log h_opt with the package's forward/backward
-   and Adam kernels (minibatch order from a seeded permutation).
-3. ``render_learned`` runs the ray loop that takes the network's step,
-   exp(-margin) h_opt, re-evaluated every ``interval`` steps and scaled with r
-   in between.  With ``check_tol`` > 0 the embedded Euler-midpoint difference
-   h |k2 - k1| guards each step: a failing proposal shrinks (twice at most),
-   then the plain step h = clamp(h_scale r, h_min, h_max) is taken.
+   accumulation) to the standardised log multiplier with the package's
+   forward/backward and Adam kernels (minibatch order from a seeded
+   permutation).
+3. ``render_learned`` runs the ray loop whose step is h_plain times the
+   network's multiplier exp(y - margin), floored at ``min_scale``, re-evaluated
+   every ``interval`` steps.  With ``check_tol`` > 0 the embedded
+   Euler-midpoint difference h |k2 - k1| checks each proposal; a failing
+   step is taken by the step-doubling controller (``fallback="controller"``)
+   or is the plain step (``fallback="plain"``).  ``brick_scale`` > 0 caps
+   steps inside the coefficient brick at that multiple of h_plain, so the
+   radiative transfer is resolved as finely as the plain method at
+   brick_scale times its step.
 
 The plain fixed-step RK2 method stays the reference: ``render_plain`` and the
 FP64 kernel at a finer step judge the learned method's image error.
@@ -22,6 +28,7 @@ FP64 kernel at a finer step judge the learned method's image error.
 from __future__ import annotations
 
 import ctypes
+import json
 import math
 from dataclasses import dataclass, replace
 from pathlib import Path
@@ -35,10 +42,11 @@ from . import _lib
 from .render import DeviceBrick, RenderConfig, Renderer, View
 
 N_FEATURES = 8
-FEATURE_NAMES = ("log_r", "cos_theta", "p_r", "p_theta", "spin_a", "log_abs_delta", "p_phi", "log_jI")
+FEATURE_NAMES = ("log_r", "cos_theta", "asinh_p_r", "asinh_p_theta", "spin_a", "log_abs_delta", "p_phi", "log_jI")
 # The spin feature is standardised with a fixed scale: training scenes span a
 # narrow band of spins and the data spread would magnify any other spin.
 FIXED_NORM = {4: (0.5, 0.5)}
+FALLBACKS = {"plain": 0, "controller": 1}
 WEIGHTS_DIR = Path(__file__).resolve().parent / "weights"
 
 
@@ -52,31 +60,47 @@ class AdaptStruct(ctypes.Structure):
         ("h_ceil", ctypes.c_float),
         ("margin", ctypes.c_float),
         ("check_tol", ctypes.c_float),
+        ("brick_scale", ctypes.c_float),
+        ("min_scale", ctypes.c_float),
         ("interval", ctypes.c_int32),
         ("max_attempts", ctypes.c_int32),
+        ("fallback", ctypes.c_int32),
         ("seed", ctypes.c_uint32),
     ]
 
 
 @dataclass(frozen=True)
 class AdaptConfig:
+    """Parameters of the step-doubling controller and of the learned loop
+    (``bhn_adapt_params``).  The defaults are the learned loop's measured
+    operating point: proposals at the network's h_opt (margin 0) with a floor
+    of 0.3 plain steps, network evaluated every 4 steps, Euler-midpoint check
+    at 1e-3 with the controller as fallback, in-brick steps no longer than
+    the plain step."""
+
     tol: float = 1e-4
     sample_prob: float = 0.0
     h_floor: float = 1e-6
     h_ceil: float = 64.0
     margin: float = 0.0
-    check_tol: float = 0.0
+    check_tol: float = 1e-3
+    brick_scale: float = 1.0
+    min_scale: float = 0.3
     interval: int = 4
     max_attempts: int = 16
+    fallback: str = "controller"   # learned: "plain" or "controller" takes a step that fails the check
     seed: int = 1
 
     def to_struct(self) -> AdaptStruct:
+        if self.fallback not in FALLBACKS:
+            raise ValueError(f"fallback must be one of {sorted(FALLBACKS)}")
         s = AdaptStruct()
-        s.tol, s.sample_prob, s.h_floor, s.h_ceil, s.margin = (float(self.tol), float(self.sample_prob),
-                                                               float(self.h_floor), float(self.h_ceil),
-                                                               float(self.margin))
-        s.check_tol = float(self.check_tol)
-        s.interval, s.max_attempts, s.seed = int(self.interval), int(self.max_attempts), int(self.seed) & 0xFFFFFFFF
+        s.tol, s.sample_prob, s.h_floor, s.h_ceil = (float(self.tol), float(self.sample_prob), float(self.h_floor),
+                                                     float(self.h_ceil))
+        s.margin, s.check_tol, s.brick_scale, s.min_scale = (float(self.margin), float(self.check_tol),
+                                                             float(self.brick_scale), float(self.min_scale))
+        s.interval, s.max_attempts, s.fallback = int(self.interval), int(self.max_attempts), FALLBACKS[self.fallback]
+        s.seed = int(self.seed) & 0xFFFFFFFF
         return s
 
 
@@ -112,6 +136,7 @@ class StepNet:
     params: torch.Tensor          # (bhn_mlp_param_count,) float32 on the device
     norm: np.ndarray              # 18 floats: mu_x[8], 1/sigma_x[8], mu_y, sigma_y
     losses: list[float] | None = None
+    meta: dict | None = None      # provenance of trained weights (samples, scene seed, tolerance)
     _blob: torch.Tensor | None = None
 
     @classmethod
@@ -139,14 +164,16 @@ class StepNet:
 
     def save(self, path) -> None:
         np.savez_compressed(path, params=self.params.cpu().numpy(), norm=self.norm,
-                            losses=np.asarray(self.losses or [], dtype=np.float64))
+                            losses=np.asarray(self.losses or [], dtype=np.float64),
+                            meta=np.asarray(json.dumps(self.meta or {})))
 
     @classmethod
     def load(cls, path, device=None) -> "StepNet":
         device = device or dev.require_cuda()
         with np.load(path) as z:
+            meta = json.loads(str(z["meta"])) if "meta" in z else None
             return cls(torch.from_numpy(z["params"]).to(device), z["norm"].astype(np.float32),
-                       list(z["losses"]) if "losses" in z else None)
+                       [float(x) for x in z["losses"]] if "losses" in z else None, meta)
 
     def infer(self, features_std: torch.Tensor) -> torch.Tensor:
         """The in-kernel inference path on standardised feature rows (test hook)."""
@@ -158,7 +185,7 @@ class StepNet:
 
 
 def compute_norm(samples: torch.Tensor) -> np.ndarray:
-    """Standardisation of the 8 features and of log h from the sample rows."""
+    """Standardisation of the 8 features and of the log multiplier from the sample rows."""
     s = samples.double()
     mu = s.mean(dim=0).cpu().numpy()
     sd = s.std(dim=0).cpu().numpy()
@@ -201,29 +228,36 @@ class MethodRun:
 
 def render_adaptive(brick: DeviceBrick, views: Sequence[View], adapt: AdaptConfig, *, samples: torch.Tensor | None = None,
                     sample_count: torch.Tensor | None = None, config: RenderConfig | None = None,
-                    ray_outputs: bool = False) -> MethodRun:
-    """Step-doubling controller over the views (optionally recording samples)."""
+                    ray_outputs: bool = False, repeats: int = 1) -> MethodRun:
+    """Step-doubling controller over the views (optionally recording samples;
+    fastest of ``repeats`` launches, which then record samples repeatedly)."""
     L = _declare()
     rnd = Renderer(brick, views, config=config or RenderConfig(256, 4, 4, 8, 32), precision="fp32",
                    ray_outputs=ray_outputs)
-    counters = torch.zeros(4, dtype=torch.int64, device=brick.device)
     st = adapt.to_struct()
     cap = 0 if samples is None else samples.shape[0]
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    _lib.check(L.bhn_adaptive_launch(*_launch_args(rnd), ctypes.byref(st), dev.ptr(samples), dev.ptr(sample_count),
-                                     cap, dev.ptr(counters), dev.stream_ptr()))
-    b.record()
-    b.synchronize()
-    c = counters.cpu().tolist()
-    return MethodRun(rnd, {"stage_pairs": c[0], "accepted": c[1], "rejected": c[2]}, a.elapsed_time(b))
+    best, counters_out = float("inf"), None
+    for _ in range(max(1, repeats)):
+        counters = torch.zeros(4, dtype=torch.int64, device=brick.device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        _lib.check(L.bhn_adaptive_launch(*_launch_args(rnd), ctypes.byref(st), dev.ptr(samples),
+                                         dev.ptr(sample_count), cap, dev.ptr(counters), dev.stream_ptr()))
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        if ms < best:
+            best = ms
+            c = counters.cpu().tolist()
+            counters_out = {"rhs_evals": c[0], "steps": c[1], "rejected": c[2]}
+    return MethodRun(rnd, counters_out, best)
 
 
 def render_learned(brick: DeviceBrick, views: Sequence[View], net: StepNet, adapt: AdaptConfig, *,
                    config: RenderConfig | None = None, ray_outputs: bool = False, repeats: int = 1) -> MethodRun:
     """The ray loop with the network's step proposal (fastest of ``repeats`` launches)."""
     L = _declare()
-    rnd = Renderer(brick, views, config=config or RenderConfig(128, 8, 4, 8, 32), precision="fp32",
+    rnd = Renderer(brick, views, config=config or RenderConfig(128, 5, 4, 8, 32), precision="fp32",
                    ray_outputs=ray_outputs)
     blob = net.blob()
     st = adapt.to_struct()
@@ -263,8 +297,17 @@ def render_plain(brick: DeviceBrick, views: Sequence[View], *, precision: str = 
     return MethodRun(rnd, {"steps": st.ray_steps, "rhs_evals": 2 * st.ray_steps}, best)
 
 
+def count_samples(brick: DeviceBrick, views: Sequence[View], adapt: AdaptConfig) -> int:
+    """How many rows the controller would record with ``adapt`` (a dry run
+    into a one-row buffer: the device counter keeps counting past capacity)."""
+    row = torch.empty((1, 9), dtype=torch.float32, device=brick.device)
+    count = torch.zeros(1, dtype=torch.int64, device=brick.device)
+    render_adaptive(brick, views, adapt, samples=row, sample_count=count)
+    return int(count.item())
+
+
 def generate_samples(brick: DeviceBrick, views: Sequence[View], adapt: AdaptConfig, capacity: int) -> torch.Tensor:
-    """Run the controller and return the recorded (features, log h) rows."""
+    """Run the controller and return the recorded (features, log multiplier) rows."""
     samples = torch.empty((capacity, 9), dtype=torch.float32, device=brick.device)
     count = torch.zeros(1, dtype=torch.int64, device=brick.device)
     render_adaptive(brick, views, adapt, samples=samples, sample_count=count)
@@ -274,7 +317,7 @@ def generate_samples(brick: DeviceBrick, views: Sequence[View], adapt: AdaptConf
 
 def train(samples: torch.Tensor, *, epochs: int = 6, batch: int = 4096, lr: float = 2e-3, seed: int = 0,
           net: StepNet | None = None, log=None) -> StepNet:
-    """Fit the network to standardised log h with the package's kernels."""
+    """Fit the network to the standardised log multiplier with the package's kernels."""
     L = _declare()
     device = samples.device
     norm = compute_norm(samples) if net is None else net.norm

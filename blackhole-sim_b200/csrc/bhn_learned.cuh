@@ -6,9 +6,10 @@
 //     Richardson estimate |y_{h/2,h/2} - y_h| / 3 in a mixed norm decides
 //     acceptance, and h is rescaled by 0.9 err^(-1/3) (clamped).  Accepted
 //     steps are recorded, with a hash-chosen probability, as training samples:
-//     8 features of the state at the step start and log h_opt, where
-//     h_opt = h err^(-1/3) is the step whose estimated RK2 error (O(h^3)) is
-//     exactly the tolerance.  h_opt is a function of the local state alone,
+//     8 features of the state at the step start and log(h_opt / h_plain),
+//     where h_opt = h err^(-1/3) is the step whose estimated RK2 error (O(h^3))
+//     is exactly the tolerance and h_plain = clamp(h_scale r, h_min, h_max)
+//     the plain step there.  h_opt is a function of the local state alone,
 //     unlike the accepted h, which lags the controller's history; a network
 //     fitted to the accepted h and fed its own previous proposal drifts.  The
 //     kernel also renders the adaptive image with the brick accumulation of
@@ -20,12 +21,16 @@
 //   * learned_kernel: the ray loop with the network's proposal.  A warp
 //     evaluates the network for its 32 rays with warp-level BF16
 //     mma.sync.m16n8k16 (two m16 row tiles; each layer's accumulator tiles are
-//     the next layer's A fragments), every `interval` steps; in between the
-//     proposal scales with r.  An embedded Euler-vs-midpoint estimate
-//     h |k2 - k1| (O(h^2)) guards every step against gross mispredictions:
-//     a proposal that fails its check tolerance is shrunk by
-//     0.9 e^(-1/2) (at least to a tenth) up to twice, then replaced by the
-//     plain step h = clamp(h_scale r, h_min, h_max).
+//     the next layer's A fragments), every `interval` steps.  The network
+//     predicts log(h_opt / h_plain), the multiplier on the plain step at the
+//     current r, floored at min_scale.  An embedded Euler-vs-midpoint
+//     estimate h |k2 - k1| (O(h^2), two RHS evaluations like the plain step)
+//     checks every proposal; where it fails (the network mispredicts, e.g.
+//     rays grazing the spin axis) either the plain step (fallback 0) or the
+//     step-doubling controller, started from 0.9 e^(-1/2) h (fallback 1),
+//     takes that step.
+//   * Both tracers cap steps inside the brick (brick_limit) and keep the
+//     plain tracers' horizon guard (crosses_horizon).
 
 namespace bhn {
 
@@ -339,8 +344,11 @@ struct AdaptParams {
     float h_floor, h_ceil;
     float margin;       // learned: log-h safety margin subtracted from the proposal
     float check_tol;    // learned: tolerance of the embedded check (0: no check)
+    float brick_scale;  // in-brick step cap as a multiple of the plain step (0: none)
+    float min_scale;    // learned: the step is at least min_scale times the plain step
     int interval;       // learned: steps between network evaluations
     int max_attempts;   // adaptive: attempts per step before forcing acceptance
+    int fallback;       // learned: a failed check takes the plain step (0) or the controller's (1)
     uint32_t seed;
 };
 
@@ -361,6 +369,44 @@ __device__ __forceinline__ void rk2_stages(const Geo &g, float h, const StepCons
     sincos_pole(dm, south, s, c);
     rhs32(fmaf(hh, k1.r, r0), fmaf(hh, k1.r, x0), s, c, fmaf(hh, k1.pr, g.pr), fmaf(hh, k1.pth, g.pth), pt, pphi,
           C.a, C.a2, C.dpm, k2);
+}
+
+__device__ __forceinline__ void rk2_k1(const Geo &g, const StepConst &C, float pt, float pphi, Deriv32 &k1) {
+    const bool south = g.th_h > kHalfPiF;
+    const float d0 = south ? (kPiH - g.th_h) + (kPiL - g.th_l) : g.th_h + g.th_l;
+    float s, c;
+    sincos_pole(d0, south, s, c);
+    rhs32(g.rh + g.rl, (g.rh - C.rp_h) + (g.rl - C.rp_l), s, c, g.pr, g.pth, pt, pphi, C.a, C.a2, C.dpm, k1);
+}
+
+// Radiative-transfer limit of an error-controlled step.  The coefficient
+// brick is sampled once per step at the step's midpoint (the plain method's
+// rule), so its resolution is set by the step length, which the geodesic error
+// norm does not see: inside the brick's (r, theta) box the step is capped at
+// brick_scale times the plain step h = clamp(h_scale r, h_min, h_max); outside
+// it, a step that would enter the box along k1 ends at most one such step
+// past the entry point.  brick_scale <= 0 disables the limit.
+__device__ __forceinline__ float brick_limit(float h, const Geo &g, const Deriv32 &k1, const StepConst &C,
+                                             const Tables &T, int nr, int nt, float brick_scale) {
+    if (!(brick_scale > 0.0f)) return h;
+    const float r = g.rh + g.rl, th = g.th_h + g.th_l;
+    const float r_in = T.grf[0], r_out = T.grf[nr - 1], t_lo = T.gtf[0], t_hi = T.gtf[nt - 1];
+    const float hb = brick_scale * fminf(fmaxf(C.hs * fminf(r, r_out), C.hmin), C.hmax);
+    const bool in_r = r >= r_in && r <= r_out, in_t = th >= t_lo && th <= t_hi;
+    if (in_r && in_t) return fminf(h, hb);
+    // affine time until each coordinate range is reached (0 when inside, inf when moving away)
+    float tr = 0.0f, tt = 0.0f;
+    if (!in_r) tr = r > r_out ? (k1.r < 0.0f ? (r - r_out) / -k1.r : INFINITY) : (k1.r > 0.0f ? (r_in - r) / k1.r : INFINITY);
+    if (!in_t)
+        tt = th < t_lo ? (k1.th > 0.0f ? (t_lo - th) / k1.th : INFINITY) : (k1.th < 0.0f ? (th - t_hi) / -k1.th : INFINITY);
+    return fminf(h, fmaxf(tr, tt) + hb);
+}
+
+// The plain tracers' horizon guard: the trial step's midpoint (Euler half
+// step) lies inside the horizon, so the step is not taken and the ray is
+// captured.
+__device__ __forceinline__ bool crosses_horizon(const Geo &g, const StepConst &C, float h, const Deriv32 &k1) {
+    return fmaf(0.5f * h, k1.r, (g.rh - C.rp_h) + (g.rl - C.rp_l)) < 0.0f;
 }
 
 // g + h k2 with compensated positions, theta clamp and phi kept in [0, 2 pi).
@@ -398,6 +444,35 @@ __device__ __forceinline__ float mixed_norm(float er, float eth, float eph, floa
     e = fmaxf(e, fabsf(epr) / (1.0f + fabsf(g.pr)));
     e = fmaxf(e, fabsf(epth) / (1.0f + fabsf(g.pth)));
     return e * it;
+}
+
+// Step-doubling attempts from g (k1 = the derivatives at g) with trial step h:
+// one step of h against two of h/2, Richardson estimate |y_{h/2,h/2} - y_h| / 3
+// in units of the tolerance.  Returns the two-half-step solution of the
+// accepted attempt; h is left at the accepted step and err at its estimate.
+__device__ __forceinline__ Geo doubling_step(const Geo &g, float &h, Deriv32 &k1, const StepConst &C, float pt,
+                                             float pphi, const AdaptParams &A, float &err,
+                                             unsigned long long &n_eval, unsigned long long &n_rej) {
+    Deriv32 k2;
+    rk2_stages(g, h, C, pt, pphi, k1, k2, false);
+    Geo y1 = geo_advance(g, h, k2), y2;
+    for (int attempt = 0;; ++attempt) {
+        Deriv32 k2h, k1b, k2b;
+        rk2_stages(g, 0.5f * h, C, pt, pphi, k1, k2h, false);
+        const Geo yh = geo_advance(g, 0.5f * h, k2h);
+        rk2_stages(yh, 0.5f * h, C, pt, pphi, k1b, k2b, true);
+        y2 = geo_advance(yh, 0.5f * h, k2b);
+        n_eval += 5;
+        err = mixed_norm((y2.rh - y1.rh) + (y2.rl - y1.rl), (y2.th_h - y1.th_h) + (y2.th_l - y1.th_l),
+                         (y2.ph_h - y1.ph_h) + (y2.ph_l - y1.ph_l), y2.pr - y1.pr, y2.pth - y1.pth, g, A.tol) *
+              (1.0f / 3.0f);
+        if (!(err > 1.0f) || attempt + 1 >= A.max_attempts || h <= A.h_floor) break;
+        ++n_rej;
+        h = fmaxf(h * fmaxf(0.2f, 0.9f * __powf(err, -1.0f / 3.0f)), A.h_floor);
+        rk2_stages(g, h, C, pt, pphi, k1, k2, false);
+        y1 = geo_advance(g, h, k2);
+    }
+    return y2;
 }
 
 // Uniform [0, 1) from (ray, step, seed) by a 32-bit integer hash (splitmix-style mixing).
@@ -499,8 +574,8 @@ __device__ __forceinline__ void step_features(const Geo &g, const StepConst &C, 
     const float x = (g.rh - C.rp_h) + (g.rl - C.rp_l);
     f[0] = __logf(r);
     f[1] = c;
-    f[2] = g.pr;
-    f[3] = g.pth;
+    f[2] = asinhf(g.pr);  // p_r grows like 1/Delta near the horizon
+    f[3] = asinhf(g.pth);
     f[4] = C.a;
     f[5] = __logf(fabsf(x * (x + C.dpm)) + 1e-30f);
     f[6] = pphi;
@@ -621,27 +696,16 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
                     st = BHN_RAY_CAPTURED;
                     break;
                 }
-                Deriv32 k1, k2;
-                rk2_stages(g, h, C, pt, pphi, k1, k2, true);
-                Geo y1 = geo_advance(g, h, k2), yh, y2;
-                float err = 0.0f;
-                for (int attempt = 0;; ++attempt) {
-                    Deriv32 k2h, k1b, k2b;
-                    rk2_stages(g, 0.5f * h, C, pt, pphi, k1, k2h, false);
-                    yh = geo_advance(g, 0.5f * h, k2h);
-                    rk2_stages(yh, 0.5f * h, C, pt, pphi, k1b, k2b, true);
-                    y2 = geo_advance(yh, 0.5f * h, k2b);
-                    n_eval += 5;
-                    err = mixed_norm((y2.rh - y1.rh) + (y2.rl - y1.rl), (y2.th_h - y1.th_h) + (y2.th_l - y1.th_l),
-                                     (y2.ph_h - y1.ph_h) + (y2.ph_l - y1.ph_l), y2.pr - y1.pr, y2.pth - y1.pth, g,
-                                     L.A.tol) * (1.0f / 3.0f);
-                    if (!(err > 1.0f) || attempt + 1 >= L.A.max_attempts || h <= L.A.h_floor) break;
-                    ++n_rej;
-                    h = fmaxf(h * fmaxf(0.2f, 0.9f * __powf(err, -1.0f / 3.0f)), L.A.h_floor);
-                    rk2_stages(g, h, C, pt, pphi, k1, k2, false);
-                    y1 = geo_advance(g, h, k2);
+                Deriv32 k1;
+                rk2_k1(g, C, pt, pphi, k1);
+                h = fmaxf(brick_limit(h, g, k1, C, T, P.nr, P.nt, L.A.brick_scale), L.A.h_floor);
+                if (crosses_horizon(g, C, h, k1)) {
+                    st = BHN_RAY_CAPTURED;
+                    break;
                 }
-                // record (features at the step start, log h_opt); err is floored at
+                float err = 0.0f;
+                const Geo y2 = doubling_step(g, h, k1, C, pt, pphi, L.A, err, n_eval, n_rej);
+                // record (features at the step start, log(h_opt / h_plain)); err is floored at
                 // 1e-6 so a step held back by the growth cap extrapolates at most 100x
                 if (L.samples && hash_uniform((uint32_t)slot, (uint32_t)steps, L.A.seed) < L.A.sample_prob) {
                     const unsigned long long k = atomicAdd(L.sample_count, 1ull);
@@ -652,7 +716,8 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
 #pragma unroll
                         for (int q = 0; q < 8; ++q) o[q] = f[q];
                         const float h_opt = h * __powf(fmaxf(err, 1e-6f), -1.0f / 3.0f);
-                        o[8] = __logf(fminf(fmaxf(h_opt, L.A.h_floor), L.A.h_ceil));
+                        const float h_plain = fminf(fmaxf(C.hs * (g.rh + g.rl), C.hmin), C.hmax);
+                        o[8] = __logf(fminf(fmaxf(h_opt, L.A.h_floor), L.A.h_ceil) / h_plain);
                     }
                 }
                 const float dr = (y2.rh - g.rh) + (y2.rl - g.rl), dph = (y2.ph_h - g.ph_h) + (y2.ph_l - g.ph_l);
@@ -713,7 +778,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
         px.px = px.py = 0;
         px.out_idx = 0;
         Geo g = {1000.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        float pt = -1.0f, pphi = 0.0f, h_net = 1.0f, r_net = 1.0f;
+        float pt = -1.0f, pphi = 0.0f, mult = 1.0f;
         StokesAcc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
         int steps = 0, st = -1;
         if (alive) {
@@ -734,8 +799,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
 #pragma unroll
                 for (int q = 0; q < 8; ++q) f[q] = alive ? (f[q] - N.mu_x[q]) * N.inv_sx[q] : 0.0f;
                 const float y = mlp_warp_infer(f, sb, xs, ys);
-                h_net = __expf(fmaf(N.sig_y, y, N.mu_y));
-                r_net = g.rh + g.rl;
+                mult = __expf(fmaf(N.sig_y, y, N.mu_y) - L.A.margin);
                 ++n_net;
             }
             if (!alive) continue;
@@ -745,31 +809,49 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
                 continue;
             }
             const float r0 = g.rh + g.rl;
-            // the proposal scales with r between network evaluations
-            float h = fminf(fmaxf(h_net * (r0 / r_net) * __expf(-L.A.margin), L.A.h_floor), L.A.h_ceil);
+            // the network's multiplier applies to the plain step at the current r
+            const float h_plain = fminf(fmaxf(C.hs * r0, C.hmin), C.hmax);
+            float h = fminf(fmaxf(fmaxf(mult, L.A.min_scale) * h_plain, L.A.h_floor), L.A.h_ceil);
             Deriv32 k1, k2;
-            rk2_stages(g, h, C, pt, pphi, k1, k2, true);
-            n_eval += 2;
-            if (L.A.check_tol > 0.0f) {
-                // the Euler and midpoint solutions differ by h (k2 - k1)
-                for (int tries = 0;; ++tries) {
-                    const float e = mixed_norm(h * (k2.r - k1.r), h * (k2.th - k1.th), h * (k2.ph - k1.ph),
-                                               h * (k2.pr - k1.pr), h * (k2.pth - k1.pth), g, L.A.check_tol);
-                    if (!(e > 1.0f)) break;
-                    ++n_fb;
-                    ++n_eval;
-                    if (tries == 2) {  // the plain step
-                        h = fminf(fmaxf(C.hs * r0, C.hmin), C.hmax);
-                        rk2_stages(g, h, C, pt, pphi, k1, k2, false);
-                        break;
-                    }
-                    h = fmaxf(h * fmaxf(0.1f, 0.9f * rsqrtf(e)), L.A.h_floor);
-                    rk2_stages(g, h, C, pt, pphi, k1, k2, false);
-                }
+            rk2_k1(g, C, pt, pphi, k1);
+            h = fmaxf(brick_limit(h, g, k1, C, T, P.nr, P.nt, L.A.brick_scale), L.A.h_floor);
+            if (crosses_horizon(g, C, h, k1)) {
+                st = BHN_RAY_CAPTURED;
+                alive = false;
+                continue;
             }
-            const Geo y = geo_advance(g, h, k2);
-            const float dr = (y.rh - g.rh) + (y.rl - g.rl), dph = h * k2.ph;
-            brick_segment(T, rec, P.nr, P.nt, P.np, C, g, y, dr, dph, acc);
+            rk2_stages(g, h, C, pt, pphi, k1, k2, false);
+            n_eval += 2;
+            float e = 0.0f;
+            if (L.A.check_tol > 0.0f) {
+                // the Euler and midpoint solutions differ by h (k2 - k1).  The phi
+                // difference is weighted by sin(theta) (the angle it subtends):
+                // phi is cyclic, so its error does not feed back into the motion,
+                // and near the spin axis its coordinate rate ~ 1/sin^2(theta)
+                // would otherwise fail every proposal there.
+                const float sth = fabsf(__sinf(g.th_h));
+                e = mixed_norm(h * (k2.r - k1.r), h * (k2.th - k1.th), sth * h * (k2.ph - k1.ph), h * (k2.pr - k1.pr),
+                               h * (k2.pth - k1.pth), g, L.A.check_tol);
+            }
+            Geo y;
+            if (!(e > 1.0f)) {
+                y = geo_advance(g, h, k2);
+            } else if (L.A.fallback == 0) {  // misprediction: the plain step
+                ++n_fb;
+                ++n_eval;
+                h = h_plain;
+                rk2_stages(g, h, C, pt, pphi, k1, k2, false);
+                y = geo_advance(g, h, k2);
+            } else {  // misprediction: the step-doubling controller takes this step
+                ++n_fb;
+                h = fmaxf(h * fmaxf(0.1f, 0.9f * rsqrtf(e)), L.A.h_floor);
+                float err;
+                unsigned long long n_rej = 0;
+                y = doubling_step(g, h, k1, C, pt, pphi, L.A, err, n_eval, n_rej);
+            }
+            const float dr = (y.rh - g.rh) + (y.rl - g.rl), dph = (y.ph_h - g.ph_h) + (y.ph_l - g.ph_l);
+            const float dph_u = dph > 3.14159f ? dph - kTwoPiH : (dph < -3.14159f ? dph + kTwoPiH : dph);
+            brick_segment(T, rec, P.nr, P.nt, P.np, C, g, y, dr, dph_u, acc);
             const bool finite = isfinite(y.rh + y.th_h + y.ph_h + y.pr + y.pth);
             g = y;
             ++steps;
@@ -804,8 +886,9 @@ static int learn_params(const void *records, const void *tables, int32_t nr, int
     if (rc) return rc;
     if (!ap) return fail(BHN_ERR_VALUE, "adapt params must not be NULL");
     if (!(ap->tol > 0.0f) || !(ap->h_floor > 0.0f) || !(ap->h_ceil >= ap->h_floor) || ap->interval < 1 ||
-        ap->max_attempts < 1 || !(ap->sample_prob >= 0.0f) || !(ap->check_tol >= 0.0f))
-        return fail(BHN_ERR_VALUE, "adapt params: need tol > 0, 0 < h_floor <= h_ceil, check_tol >= 0, interval >= 1, "
+        ap->max_attempts < 1 || (ap->fallback != 0 && ap->fallback != 1) || !(ap->sample_prob >= 0.0f) ||
+        !(ap->check_tol >= 0.0f) || !(ap->min_scale > 0.0f))
+        return fail(BHN_ERR_VALUE, "adapt params: need tol > 0, 0 < h_floor <= h_ceil, check_tol >= 0, min_scale > 0, "
                                    "max_attempts >= 1");
     if (n_views < 1 || !records || !tables || !out || !scratch) return fail(BHN_ERR_VALUE, "missing buffers or views");
     ScratchLayout SL = scratch_layout(n_views);
@@ -841,6 +924,9 @@ static int learn_params(const void *records, const void *tables, int32_t nr, int
     L.A.h_ceil = ap->h_ceil;
     L.A.margin = ap->margin;
     L.A.check_tol = ap->check_tol;
+    L.A.brick_scale = ap->brick_scale;
+    L.A.min_scale = ap->min_scale;
+    L.A.fallback = ap->fallback;
     L.A.interval = ap->interval;
     L.A.max_attempts = ap->max_attempts;
     L.A.seed = ap->seed;

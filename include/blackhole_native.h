@@ -237,16 +237,23 @@ typedef struct bhn_adapt_params {
     float tol;           /* mixed-norm tolerance: |e_i| <= tol (1 + |y_i|) over r, theta, phi, p_r, p_theta */
     float sample_prob;   /* controller: probability of recording an accepted step */
     float h_floor, h_ceil;
-    float margin;        /* learned: subtracted from the proposed log h */
+    float margin;        /* learned: subtracted from the network's log multiplier of the plain step */
     float check_tol;     /* learned: tolerance of the embedded Euler-midpoint check h|k2 - k1| (0: none) */
-    int32_t interval;    /* learned: steps between network evaluations (the proposal scales with r between) */
-    int32_t max_attempts;
-    uint32_t seed;
+    float brick_scale;   /* both: inside the brick's (r, theta) box the step is at most brick_scale times the
+                            plain step clamp(h_scale r, h_min, h_max), and a step entering the box ends at most
+                            one such step past the entry point (0: no limit) */
+    float min_scale;     /* learned: the step is at least min_scale times the plain step (> 0) */
+    int32_t interval;    /* learned: steps between network evaluations (the multiplier is kept in between) */
+    int32_t max_attempts; /* controller: attempts per step before the step is forced */
+    int32_t fallback;    /* learned: a step failing the check is the plain step (0) or the controller's (1) */
+    uint32_t seed;       /* controller: sample-selection hash seed */
 } bhn_adapt_params;
 
-/* Sample rows: 8 raw features (log r, cos theta, p_r, p_theta, a, log|Delta|,
- * p_phi, log(j_I + 1e-12)) followed by log h_opt, h_opt = h err^(-1/3) the step
- * at which the controller's error estimate equals the tolerance (9 floats). */
+/* Sample rows: 8 raw features (log r, cos theta, asinh p_r, asinh p_theta, a,
+ * log|Delta|, p_phi, log(j_I + 1e-12)) followed by log(h_opt / h_plain):
+ * h_opt = h err^(-1/3) is the step at which the controller's error estimate
+ * equals the tolerance, h_plain = clamp(h_scale r, h_min, h_max) the plain
+ * step at the same r (9 floats). */
 #define BHN_SAMPLE_FLOATS 9
 int64_t bhn_mlp_param_count(void);
 int64_t bhn_mlp_blob_bytes(void);
