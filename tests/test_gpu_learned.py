@@ -6,8 +6,8 @@
 * inference (warp-level BF16 mma.sync): equals the oracle's forward to 3e-2;
 * the step-doubling controller records finite samples and renders a finite
   image; training on them lowers the loss;
-* the learned ray loop stays within tolerance of the FP64 plain method at a
-  4x finer step.
+* the shipped network's ray loop matches the plain method's accuracy at h/4
+  with under a third of its RHS evaluations.
 """
 
 from __future__ import annotations
@@ -20,7 +20,6 @@ import blackhole_native as bn
 from blackhole_native import learned
 from oracle import mlp as M
 from tests.conftest import rel_l1
-from tests.test_gpu_render import conditioned_pixels
 
 pytestmark = pytest.mark.gpu
 
@@ -97,16 +96,34 @@ def test_controller_samples_and_training(scene3):
     assert run.counters["steps"] > 0
 
 
-def test_learned_loop_within_tolerance(scene3):
-    view = bn.View(96, 96, spin_a=0.998, inclination_deg=60.0, max_steps=8192, horizon_guard=True)
-    samples = learned.generate_samples(scene3, [view], learned.AdaptConfig(tol=1e-4, sample_prob=0.5), 200_000)
-    net = learned.train(samples, epochs=4, batch=2048, lr=3e-3)
-    run = learned.render_learned(scene3, [view], net, learned.AdaptConfig(tol=1e-4, margin=0.5, interval=2,
-                                                                          check_tol=1e-2))
-    img = run.image().cpu().numpy().astype(np.float64)
-    ref = bn.render(scene3, view.scaled_step(0.25), precision="fp64").image().cpu().numpy()
+def test_learned_gain_over_plain():
+    """The shipped network (trained on the seeded 256-view scene) against the
+    plain fixed step on an unseen scene (a = 0.998, 75 deg, seed-1 brick): at
+    in-brick resolution h/4, the learned loop matches the plain method at h/4
+    -- Stokes-I error against the FP64 kernel at h/16 within 1.25x (plus
+    2e-5) on the stable, converged pixels -- with under a third of its RHS
+    evaluations."""
+    from blackhole_native import studies
+
+    net = learned.shipped_weights()
+    assert net is not None, "blackhole_native/weights/step_net.npz is missing"
+    assert net.meta and net.meta["samples"] >= 5_000_000
+    db = bn.DeviceBrick(bn.torus_brick(256, 128, 256, spin_a=0.998, seed=1), precisions=("fp32", "fp64"))
+    v = bn.View(256, 256, spin_a=0.998, inclination_deg=75.0, max_steps=65536, horizon_guard=True)
+    ref = bn.render(db, v.scaled_step(1 / 16), precision="fp64").image().cpu().numpy()
+    ref8 = bn.render(db, v.scaled_step(1 / 8), precision="fp64").image().cpu().numpy()
+    perts = [bn.render(db, w, precision="fp64").image().cpu().numpy()
+             for w in (v.scaled_step(1 / 16 * (1 + 1e-6)), studies.camera_perturbed(v.scaled_step(1 / 16)))]
+    scale = studies.median_lit(ref[..., 0])
+    mask = studies.stable_mask(ref, perts, scale) & (
+        np.abs(ref8[..., 0] - ref[..., 0]) <= 1e-2 * np.abs(ref[..., 0]) + 1e-4 * scale)
+    assert mask.mean() >= 0.98
+    plain = learned.render_plain(db, [v.scaled_step(0.25)])
+    run = learned.render_learned(db, [v], net, learned.AdaptConfig(brick_scale=0.25))
+    img = run.image().cpu().numpy()
     assert np.all(np.isfinite(img))
-    cond = conditioned_pixels(scene3, view.scaled_step(0.25), ref)
-    assert cond.mean() >= 0.98
-    assert rel_l1(img[..., 0][cond], ref[..., 0][cond]) <= 2e-2
-    assert run.counters["steps"] > 0 and run.counters["net_evals_per_warp"] > 0
+    e_plain = studies.image_errors(plain.image().cpu().numpy(), ref, mask, scale)["capped_rel_l1_I"]
+    e_learn = studies.image_errors(img, ref, mask, scale)["capped_rel_l1_I"]
+    assert e_learn <= 1.25 * e_plain + 2e-5, (e_learn, e_plain)
+    assert run.counters["rhs_evals"] <= plain.counters["rhs_evals"] / 3, (run.counters, plain.counters)
+    assert run.counters["net_evals_per_warp"] > 0
