@@ -187,8 +187,9 @@ struct __align__(16) ViewDev {
     double h_scale, h_min, h_max, L, max_tau;
     double width_d, height_d;          // image size as doubles (divisors of accelerated_renderer.py:138-140)
     int32_t width, height, x0, y0, crop_w, crop_h, max_steps, has_roll;
-    int32_t valid, flags, pad[2];
-    int64_t out_offset, ray_begin, ray_count, pad2;
+    int32_t valid, flags;
+    int32_t axis_x0, axis_x1;          // crop-local columns [x0, x1) of the rays traced first (see setup_views_kernel)
+    int64_t out_offset, ray_begin, ray_count, axis_begin;
 };
 
 struct QueueState {  // at offset 0 of the render scratch
@@ -200,7 +201,7 @@ struct QueueState {  // at offset 0 of the render scratch
 static_assert(sizeof(QueueState) == 64, "queue state size");
 
 struct ScratchLayout {
-    int64_t queue, stats, raw_views, views, ray_begin, total;
+    int64_t queue, stats, raw_views, views, ray_begin, axis_begin, total;
 };
 __host__ __device__ inline ScratchLayout scratch_layout(int32_t n_views) {
     ScratchLayout L;
@@ -209,7 +210,8 @@ __host__ __device__ inline ScratchLayout scratch_layout(int32_t n_views) {
     L.raw_views = 256;
     L.views = (L.raw_views + (int64_t)sizeof(bhn_view) * n_views + 255) & ~(int64_t)255;
     L.ray_begin = (L.views + (int64_t)sizeof(ViewDev) * n_views + 255) & ~(int64_t)255;
-    L.total = (L.ray_begin + 8 * ((int64_t)n_views + 1) + 255) & ~(int64_t)255;
+    L.axis_begin = (L.ray_begin + 8 * ((int64_t)n_views + 1) + 255) & ~(int64_t)255;
+    L.total = (L.axis_begin + 8 * ((int64_t)n_views + 1) + 255) & ~(int64_t)255;
     return L;
 }
 

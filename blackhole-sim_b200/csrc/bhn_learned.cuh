@@ -908,6 +908,7 @@ static int learn_params(const void *records, const void *tables, int32_t nr, int
     P.n_views = n_views;
     P.views = reinterpret_cast<const ViewDev *>(sc + SL.views);
     P.ray_begin = reinterpret_cast<const int64_t *>(sc + SL.ray_begin);
+    P.axis_begin = reinterpret_cast<const int64_t *>(sc + SL.axis_begin);  // unused: these tracers keep the tile order
     P.q = reinterpret_cast<QueueState *>(sc + SL.queue);
     P.stats = reinterpret_cast<bhn_render_stats *>(sc + SL.stats);
     P.out = out;

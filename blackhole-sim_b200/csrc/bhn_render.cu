@@ -39,8 +39,19 @@ __device__ __forceinline__ double safe_theta(double th) {  // kerr.py:35-36
     return fmin(fmax(th, kEpsTheta), kPi - kEpsTheta);
 }
 
+// Rays with small axial angular momentum |p_phi| run first.  Only they can
+// come close to the spin axis, where the clamped sin(theta) (kerr.py:93)
+// shrinks the useful step and such rays run up to max_steps -- several times
+// longer than the rest; a persistent launch would otherwise finish with these
+// few rays alone on the GPU.  For a camera without roll, p_phi of a ray is
+// sqrt(g_phiphi) n_phi with n_phi = ndc_x tan_x / |n| (the ZAMO part cancels:
+// g_tphi + g_phiphi omega = 0), so |p_phi| < kAxisBandPphi is a band of image
+// columns; the order inside and outside the band stays the tile order.  It
+// changes which ray a warp takes when, never a ray's result.
+constexpr double kAxisBandPphi = 0.5;
+
 __global__ void setup_views_kernel(const bhn_view *__restrict__ raw, int n, ViewDev *__restrict__ views,
-                                   int64_t *__restrict__ ray_begin, QueueState *q) {
+                                   int64_t *__restrict__ ray_begin, int64_t *__restrict__ axis_begin, QueueState *q) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         bhn_view v = raw[i];
         ViewDev d;
@@ -109,17 +120,31 @@ __global__ void setup_views_kernel(const bhn_view *__restrict__ raw, int n, View
         d.max_steps = v.max_steps;
         d.out_offset = v.out_offset;
         d.ray_count = (int64_t)v.crop_w * v.crop_h;
+        // |ndc_x| < u  =>  |p_phi| <= sqrt(g_phiphi) |ndc_x| tan_x < kAxisBandPphi (|n| >= 1)
+        d.axis_x0 = d.axis_x1 = 0;
+        if (d.valid && !d.has_roll && d.crop_w > 0 && d.crop_h > 0) {
+            const double u = kAxisBandPphi / (sqrt(d.gcov33) * d.tan_x);
+            const double lo = fmax((1.0 - u) * 0.5 * d.width_d - 0.5, -1.0);
+            const double hi = fmin((1.0 + u) * 0.5 * d.width_d - 0.5, d.width_d);
+            const int c0 = (int)ceil(lo) - v.x0, c1 = (int)floor(hi) + 1 - v.x0;
+            d.axis_x0 = max(0, min(c0, v.crop_w));
+            d.axis_x1 = max(d.axis_x0, min(c1, v.crop_w));
+        }
         views[i] = d;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        int64_t acc = 0;
+        int64_t acc = 0, acc_axis = 0;
         for (int i = 0; i < n; ++i) {
             views[i].ray_begin = acc;
+            views[i].axis_begin = acc_axis;
             ray_begin[i] = acc;
+            axis_begin[i] = acc_axis;
             acc += views[i].ray_count;
+            acc_axis += (int64_t)(views[i].axis_x1 - views[i].axis_x0) * views[i].crop_h;
         }
         ray_begin[n] = acc;
+        axis_begin[n] = acc_axis;
         q->total = (unsigned long long)acc;
         q->n_views = (uint32_t)n;
     }
@@ -131,10 +156,11 @@ struct PixelRef {
     int64_t out_idx;     // index into the output image buffer
 };
 
-// Ray k of a view's crop in tile order: bands of tile_h rows, tiles of tile_w
-// columns inside a band (the last band / tile of a band may be narrower).
-__device__ __forceinline__ PixelRef pixel_of(const ViewDev &v, int64_t k, int tw, int th) {
-    const int cw = v.crop_w, ch = v.crop_h;
+// Ray k of the crop columns [cx0, cx0 + cw) of a view (all crop rows) in tile
+// order: bands of tile_h rows, tiles of tile_w columns inside a band (the last
+// band / tile of a band may be narrower).
+__device__ __forceinline__ PixelRef pixel_in_columns(const ViewDev &v, int64_t k, int cx0, int cw, int tw, int th) {
+    const int ch = v.crop_h;
     const int kk = (int)k;
     const int band_rays = th * cw;
     const int band = kk / band_rays;
@@ -143,13 +169,18 @@ __device__ __forceinline__ PixelRef pixel_of(const ViewDev &v, int64_t k, int tw
     const int tile = kb / (tw * bh);
     const int kt = kb - tile * tw * bh;
     const int tw_eff = min(tw, cw - tile * tw);
-    const int lx = tile * tw + kt % tw_eff;
+    const int lx = cx0 + tile * tw + kt % tw_eff;
     const int ly = band * th + kt / tw_eff;
     PixelRef p;
     p.px = v.x0 + lx;
     p.py = v.y0 + ly;
-    p.out_idx = v.out_offset + (int64_t)ly * cw + lx;
+    p.out_idx = v.out_offset + (int64_t)ly * v.crop_w + lx;
     return p;
+}
+
+// Ray k of a view's crop in tile order.
+__device__ __forceinline__ PixelRef pixel_of(const ViewDev &v, int64_t k, int tw, int th) {
+    return pixel_in_columns(v, k, 0, v.crop_w, tw, th);
 }
 
 // kerr.py:188-233 for pixel (px, py) of a view: returns covariant momenta and
@@ -207,6 +238,7 @@ struct RenderParams {
     int nr, nt, np, n_views;
     const ViewDev *views;
     const int64_t *ray_begin;
+    const int64_t *axis_begin;  // prefix of the views' axis-band rays
     QueueState *q;
     bhn_render_stats *stats;
     void *out;
@@ -225,6 +257,39 @@ __device__ __forceinline__ int find_view(const int64_t *begin, int n, int64_t sl
         else hi = mid;
     }
     return lo;
+}
+
+// Largest i with ray_begin[i] - axis_begin[i] <= slot (the views' rays outside
+// their axis bands, view after view).
+__device__ __forceinline__ int find_view_rest(const int64_t *ray_begin, const int64_t *axis_begin, int n,
+                                              int64_t slot) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (ray_begin[mid] - axis_begin[mid] <= slot) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Queue slot -> (view, pixel) of the render kernel: first the axis-band rays of
+// every view, then every view's remaining rays (left of the band, then right).
+__device__ __forceinline__ PixelRef ordered_pixel(const ViewDev *views, const int64_t *ray_begin,
+                                                  const int64_t *axis_begin, int n, int64_t slot, int tw, int th,
+                                                  int &vi) {
+    const int64_t n_axis = axis_begin[n];
+    if (slot < n_axis) {
+        vi = n == 1 ? 0 : find_view(axis_begin, n, slot);
+        const ViewDev &v = views[vi];
+        return pixel_in_columns(v, slot - axis_begin[vi], v.axis_x0, v.axis_x1 - v.axis_x0, tw, th);
+    }
+    const int64_t s = slot - n_axis;
+    vi = n == 1 ? 0 : find_view_rest(ray_begin, axis_begin, n, s);
+    const ViewDev &v = views[vi];
+    const int64_t k = s - (ray_begin[vi] - axis_begin[vi]);
+    const int64_t left = (int64_t)v.axis_x0 * v.crop_h;
+    if (k < left) return pixel_in_columns(v, k, 0, v.axis_x0, tw, th);
+    return pixel_in_columns(v, k - left, v.axis_x1, v.crop_w - v.axis_x1, tw, th);
 }
 
 // v as an unevaluated float pair hi + lo (hi = v rounded, lo = the remainder).
@@ -811,7 +876,7 @@ __host__ __device__ inline int64_t align16(int64_t x) { return (x + 15) & ~(int6
 // Shared-memory layout of the persistent kernel.
 __host__ __device__ inline int64_t smem_bytes(int tables_bytes, int n_views) {
     return align16(tables_bytes) + align16(8 * ((int64_t)n_views + 1)) + (int64_t)sizeof(StepConst) * n_views +
-           align16(sizeof(BlockCounters));
+           align16(sizeof(BlockCounters)) + align16(8 * ((int64_t)n_views + 1));
 }
 
 // ------------------------------------------------------------ persistent loop
@@ -823,12 +888,16 @@ __global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P)
     int64_t *vbegin = reinterpret_cast<int64_t *>(smem + align16(P.tables_bytes));
     StepConst *sconst = reinterpret_cast<StepConst *>(smem + align16(P.tables_bytes) + align16(8 * (P.n_views + 1)));
     BlockCounters *bc = reinterpret_cast<BlockCounters *>(sconst + P.n_views);
+    int64_t *abegin = reinterpret_cast<int64_t *>(reinterpret_cast<unsigned char *>(bc) + align16(sizeof(BlockCounters)));
     // grid tables, the view prefix and the per-view step constants stay in shared memory for the launch
     {
         const int4 *src = reinterpret_cast<const int4 *>(P.tables);
         int4 *dst = reinterpret_cast<int4 *>(smem);
         for (int i = threadIdx.x; i < P.tables_bytes / 16; i += blockDim.x) dst[i] = src[i];
-        for (int i = threadIdx.x; i <= P.n_views; i += blockDim.x) vbegin[i] = P.ray_begin[i];
+        for (int i = threadIdx.x; i <= P.n_views; i += blockDim.x) {
+            vbegin[i] = P.ray_begin[i];
+            abegin[i] = P.axis_begin[i];
+        }
         if (threadIdx.x == 0) memset(bc, 0, sizeof(BlockCounters));
     }
     __syncthreads();
@@ -877,9 +946,9 @@ __global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P)
         if (base >= total) break;
         const unsigned long long slot = base + lane;
         if (slot < total) {
-            const int vi = P.n_views == 1 ? 0 : find_view(vbegin, P.n_views, (int64_t)slot);
+            int vi;
+            const PixelRef px = ordered_pixel(P.views, vbegin, abegin, P.n_views, (int64_t)slot, P.tile_w, P.tile_h, vi);
             const ViewDev &v = P.views[vi];
-            const PixelRef px = pixel_of(v, (int64_t)slot - vbegin[vi], P.tile_w, P.tile_h);
             if (v.valid && v.max_steps > 0) {
                 tr.init(v, vi, px.px, px.py, px.out_idx);
                 const StepConst &C = sconst[vi];
@@ -928,9 +997,10 @@ __global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P)
             if (!alive) {
                 const unsigned long long slot = base + __popc(dead & lt_mask);
                 if (slot < total) {
-                    const int vi = P.n_views == 1 ? 0 : find_view(vbegin, P.n_views, (int64_t)slot);
+                    int vi;
+                    const PixelRef px =
+                        ordered_pixel(P.views, vbegin, abegin, P.n_views, (int64_t)slot, P.tile_w, P.tile_h, vi);
                     const ViewDev &v = P.views[vi];
-                    const PixelRef px = pixel_of(v, (int64_t)slot - vbegin[vi], P.tile_w, P.tile_h);
                     if (v.valid && v.max_steps > 0) {
                         tr.init(v, vi, px.px, px.py, px.out_idx);
                         alive = true;
@@ -1028,6 +1098,7 @@ static int launch_render(const void *records, const void *tables, int32_t nr, in
     P.n_views = n_views;
     P.views = reinterpret_cast<const ViewDev *>(sc + L.views);
     P.ray_begin = reinterpret_cast<const int64_t *>(sc + L.ray_begin);
+    P.axis_begin = reinterpret_cast<const int64_t *>(sc + L.axis_begin);
     P.q = reinterpret_cast<QueueState *>(sc + L.queue);
     P.stats = stats ? stats : reinterpret_cast<bhn_render_stats *>(sc + L.stats);
     P.out = out;
@@ -1098,6 +1169,7 @@ int bhn_render_prepare(const bhn_view *h_views, int32_t n_views, void *scratch, 
     setup_views_kernel<<<1, 256, 0, s>>>(reinterpret_cast<const bhn_view *>(sc + L.raw_views), n_views,
                                          reinterpret_cast<ViewDev *>(sc + L.views),
                                          reinterpret_cast<int64_t *>(sc + L.ray_begin),
+                                         reinterpret_cast<int64_t *>(sc + L.axis_begin),
                                          reinterpret_cast<QueueState *>(sc + L.queue));
     BHN_LAUNCH_CHECK("setup_views_kernel");
     return BHN_OK;

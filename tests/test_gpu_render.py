@@ -164,6 +164,34 @@ def test_batched_views_equal_single_views(scene_brick):
     assert sum(st.status.values()) == st.rays
 
 
+@pytest.mark.parametrize("cfg", [bn.RenderConfig(256, 4, 4, 8, 32), bn.RenderConfig(128, 4, 4, 8, 1)])
+def test_axis_band_order_traces_every_pixel_once(scene_brick, cfg):
+    """The render kernel hands out each view's small-|p_phi| column band first.
+    Views whose crops lie across, inside and outside that band, a rolled view
+    (no band) and a narrow full-width view must each have every pixel traced
+    exactly once: per-pixel outputs preset to -1 are all overwritten, and the
+    batched launch equals the views rendered one by one."""
+    b, db = scene_brick
+    views = [bn.View(1024, 1024, crop=(480, 300, 70, 9), max_steps=1500),      # across the band
+             bn.View(1024, 1024, crop=(508, 600, 6, 13), max_steps=1500),      # inside it
+             bn.View(1024, 1024, crop=(40, 40, 33, 7), max_steps=1500),        # left of it
+             bn.View(1024, 1024, crop=(900, 70, 21, 5), max_steps=1500),       # right of it
+             bn.View(64, 48, roll_deg=20.0, max_steps=1500),                   # rolled: no band
+             bn.View(97, 3, inclination_deg=60.0, max_steps=1500)]             # band of a few columns
+    r = bn.Renderer(db, views, config=cfg, ray_outputs=True)
+    r.steps.fill_(-1)
+    r.out.fill_(float("nan"))
+    res = r.launch()
+    assert int((r.steps < 0).sum()) == 0
+    assert torch.isfinite(r.out).all()
+    st = res.stats()
+    assert st.rays == sum(v.pixels for v in views) and st.ray_steps == int(r.steps.to(torch.int64).sum())
+    for i, v in enumerate(views):
+        single = bn.render(db, v, precision="fp32", config=cfg, ray_outputs=True)
+        assert torch.equal(res.image(i), single.image())
+        assert torch.equal(res.per_ray("steps", i), single.per_ray("steps"))
+
+
 @pytest.mark.parametrize("cfg", [bn.RenderConfig(64, 8, 1, 1, 32), bn.RenderConfig(256, 2, 16, 2, 8),
                                  bn.RenderConfig(128, 4, 4, 8, 1)])
 def test_launch_shape_does_not_change_pixels(scene_brick, cfg):
