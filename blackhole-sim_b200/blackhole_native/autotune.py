@@ -26,7 +26,7 @@ CACHE = Path(os.environ.get("BHN_AUTOTUNE_CACHE", Path(__file__).resolve().paren
 
 DEFAULT_SPACE = {
     "block_threads": (64, 128, 256),
-    "blocks_per_sm": (2, 4, 8),
+    "blocks_per_sm": (2, 3, 4, 6, 8),
     "tile": ((8, 4), (4, 8), (16, 2), (32, 1)),
     "refill_min": (1, 8, 16, 32),
     "reg_cap": (0, 80, 64),
@@ -59,13 +59,16 @@ def store(workload: str, config: RenderConfig, ms: float, device: torch.device, 
 
 
 def launch_candidates(space: dict | None = None, base: RenderConfig | None = None) -> Iterable[RenderConfig]:
-    """Stage 1: threads per block x resident blocks x register budget."""
+    """Stage 1: threads per block x resident blocks x register budget, each in
+    both loop modes (per-step refill and whole-warp batches), since the best
+    shape differs between them."""
     s = space or DEFAULT_SPACE
     b = base or RenderConfig()
-    for bt, bps, rc in itertools.product(s["block_threads"], s["blocks_per_sm"], s["reg_cap"]):
+    for bt, bps, rc, rm in itertools.product(s["block_threads"], s["blocks_per_sm"], s["reg_cap"],
+                                             sorted({min(s["refill_min"]), 32})):
         if bt * bps > 2048:   # more threads than an SM holds
             continue
-        yield replace(b, block_threads=bt, blocks_per_sm=bps, reg_cap=rc)
+        yield replace(b, block_threads=bt, blocks_per_sm=bps, reg_cap=rc, refill_min=rm)
 
 
 def order_candidates(space: dict | None = None, base: RenderConfig | None = None) -> Iterable[RenderConfig]:

@@ -141,30 +141,25 @@ __device__ __forceinline__ int locate_phi(const double *g, int n, double p, int 
 
 // The FP32 kernel's locators: the same searches over the float32 knots (exact
 // for the float32 midpoints the FP32 kernel samples at).
+// The closed-form guess of a uniform or geometric axis is within one cell of
+// the answer: build_tables_kernel only classifies an axis so when every knot
+// lies within a quarter cell of its model, which with FP32 rounding of the
+// guess (~1e-4 cell) keeps floor(guess) in {i - 1, i, i + 1}; one step each
+// way then gives searchsorted(side="right") - 1 exactly, without a loop.
 __device__ __forceinline__ int locate_linear_f(const float *g, int n, float x, int kind, float off, float inv) {
-    int i;
-    if (kind == kSearch) {
-        i = search_right(g, 0, n, x) - 1;
-    } else {
-        const float f = kind == kUniform ? fmaf(x, inv, -off) : fmaf(__logf(x), inv, -off);
-        i = (int)fmaxf(f, 0.0f);
-    }
-    i = max(0, min(i, n - 2));
-    while (i > 0 && x < g[i]) --i;
-    while (i < n - 2 && x >= g[i + 1]) ++i;
+    if (kind == kSearch) return max(0, min(search_right(g, 0, n, x) - 1, n - 2));
+    const float f = kind == kUniform ? fmaf(x, inv, -off) : fmaf(__logf(x), inv, -off);
+    int i = max(0, min((int)fmaxf(f, 0.0f), n - 2));
+    i -= (i > 0 && x < g[i]) ? 1 : 0;
+    i += (i < n - 2 && x >= g[i + 1]) ? 1 : 0;
     return i;
 }
 
 __device__ __forceinline__ int locate_phi_f(const float *g, int n, float p, int kind, float off, float inv) {
-    int i;
-    if (kind == kSearch) {
-        i = search_right(g, 0, n, p) - 1;
-    } else {
-        i = (int)fmaxf(fmaf(p, inv, -off), 0.0f);
-    }
-    i = max(0, min(i, n - 1));
-    while (i > 0 && p < g[i]) --i;
-    while (i < n - 1 && p >= g[i + 1]) ++i;
+    if (kind == kSearch) return max(0, min(search_right(g, 0, n, p) - 1, n - 1));
+    int i = max(0, min((int)fmaxf(fmaf(p, inv, -off), 0.0f), n - 1));
+    i -= (i > 0 && p < g[i]) ? 1 : 0;
+    i += (i < n - 1 && p >= g[i + 1]) ? 1 : 0;
     return i;
 }
 
