@@ -19,7 +19,7 @@ REPO = ROOT.parent
 CSRC = ROOT / "csrc"
 INCLUDE = REPO / "include"
 LIB = PKG / "libbhnative.so"
-SOURCES = ["bhn_api.cu", "bhn_render.cu", "bhn_noalloc.cu"]
+SOURCES = ["bhn_api.cu", "bhn_render.cu", "bhn_noalloc.cu", "bhn_synchrotron.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

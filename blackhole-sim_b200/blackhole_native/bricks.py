@@ -35,6 +35,19 @@ def horizon_radius(a: float) -> float:
     return 1.0 + math.sqrt(1.0 - a * a)
 
 
+def validate_grid(name: str, grid) -> np.ndarray:
+    """A brick axis as contiguous float64: 1-D, >= 2 finite, strictly increasing
+    values (the reference's messages, lib.rs:112-169)."""
+    g = np.ascontiguousarray(np.asarray(grid, dtype=np.float64))
+    if g.ndim != 1 or g.size < 2:
+        raise ValueError(f"{name} grid must contain at least 2 values")
+    if not np.all(np.isfinite(g)):
+        raise ValueError(f"{name} grid must contain only finite values")
+    if np.any(np.diff(g) <= 0.0):
+        raise ValueError(f"{name} grid must be strictly increasing")
+    return g
+
+
 @dataclass(frozen=True)
 class BrickGrid:
     """Host-side coefficient brick: grids plus ``[nr][nt][np][11]`` coefficients."""
@@ -47,14 +60,7 @@ class BrickGrid:
 
     def __post_init__(self) -> None:
         for name in ("r", "theta", "phi"):
-            g = np.ascontiguousarray(np.asarray(getattr(self, name), dtype=np.float64))
-            if g.ndim != 1 or g.size < 2:
-                raise ValueError(f"{name} grid must contain at least 2 values")
-            if not np.all(np.isfinite(g)):
-                raise ValueError(f"{name} grid must contain only finite values")
-            if np.any(np.diff(g) <= 0.0):
-                raise ValueError(f"{name} grid must be strictly increasing")
-            object.__setattr__(self, name, g)
+            object.__setattr__(self, name, validate_grid(name, getattr(self, name)))
         c = np.asarray(self.coeffs)
         expected = (self.r.size, self.theta.size, self.phi.size, len(COEFF_NAMES))
         if c.shape != expected:

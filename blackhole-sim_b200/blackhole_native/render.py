@@ -27,7 +27,7 @@ import torch
 
 from . import _device as dev
 from . import _lib
-from .bricks import BrickGrid, horizon_radius
+from .bricks import BrickGrid, horizon_radius, validate_grid
 
 FOV_20M_AT_1000M = 2.0 * math.degrees(math.atan(20.0 / 1000.0))  # +-20 M field of view at r_obs = 1000 M
 EPS_THETA = 1.0e-7
@@ -143,11 +143,32 @@ class DeviceBrick:
     """
 
     def __init__(self, brick: BrickGrid, device: torch.device | None = None, precisions: Sequence[str] = ("fp32",)):
+        self._init_grids(brick.r, brick.theta, brick.phi, brick.spin_a, device)
+        coeffs = dev.to_device(brick.coeffs.reshape(-1), self.device)
+        for p in precisions:
+            self._pack(coeffs, p)
+
+    @classmethod
+    def from_device_coeffs(cls, r, theta, phi, coeffs: torch.Tensor, spin_a: float = 0.0,
+                           precisions: Sequence[str] = ("fp32",)) -> "DeviceBrick":
+        """A brick whose [nr][nt][np][11] values already live on the device
+        (float32 or float64 tensor), packed without a host copy."""
+        grids = [validate_grid(n, g) for n, g in (("r", r), ("theta", theta), ("phi", phi))]
+        obj = cls.__new__(cls)
+        obj._init_grids(*grids, spin_a, coeffs.device)
+        if coeffs.numel() != obj.cells * 11 or coeffs.dtype not in (torch.float32, torch.float64):
+            raise ValueError(f"coeffs must contain exactly r*theta*phi*11 float values; expected {obj.cells * 11}")
+        flat = coeffs.contiguous().reshape(-1)
+        for p in precisions:
+            obj._pack(flat, p)
+        return obj
+
+    def _init_grids(self, r, theta, phi, spin_a, device) -> None:
         self.device = device or dev.require_cuda()
-        self.nr, self.nt, self.np = int(brick.r.size), int(brick.theta.size), int(brick.phi.size)
+        self.nr, self.nt, self.np = int(r.size), int(theta.size), int(phi.size)
         self.shape = (self.nr, self.nt, self.np)
-        self.spin_a = float(brick.spin_a)
-        self.host_grids = (brick.r, brick.theta, brick.phi)
+        self.spin_a = float(spin_a)
+        self.host_grids = (r, theta, phi)
         self.grids = [dev.to_device(g, self.device) for g in self.host_grids]
         L = _lib.lib()
         nbytes = int(L.bhn_brick_tables_bytes(self.nr, self.nt, self.np))
@@ -155,9 +176,6 @@ class DeviceBrick:
         _lib.check(L.bhn_brick_build_tables(dev.ptr(self.grids[0]), self.nr, dev.ptr(self.grids[1]), self.nt,
                                             dev.ptr(self.grids[2]), self.np, dev.ptr(self.tables), dev.stream_ptr()))
         self._records: dict[str, torch.Tensor] = {}
-        coeffs = dev.to_device(brick.coeffs.reshape(-1), self.device)
-        for p in precisions:
-            self._pack(coeffs, p)
 
     @property
     def cells(self) -> int:

@@ -224,7 +224,7 @@ int bhn_render_noalloc(const void *records, const void *tables, int32_t nr, int3
                        const bhn_view *h_views, int32_t n_views, const bhn_render_config *cfg, void *out,
                        const bhn_ray_outputs *ray_out, bhn_render_stats *stats, void *stream);
 
-/* ---- learned step-size proposal (BASELINE config 5; no reference counterpart) ----
+/* ---- learned step-size proposal (no reference counterpart) ----
  * The plain method is kerr.py:337-384's loop with the RK2 step of
  * native/cuda/kerr_stokes_kernel.cu:13 at h = clamp(h_scale r, h_min, h_max).
  * These entry points add (1) an RK2 step-doubling controller that renders the
@@ -285,6 +285,32 @@ int bhn_learned_launch(const void *records, const void *tables, int32_t nr, int3
                        const bhn_render_config *cfg, void *out, const bhn_ray_outputs *ray_out, void *scratch,
                        int64_t scratch_bytes, const bhn_adapt_params *params, const void *blob,
                        unsigned long long *counters, void *stream);
+
+/* ---- coefficient-brick precompute --------------------------------------------
+ * Replaces precompute_coefficient_bricks (python/blackhole_sim/
+ * coefficient_bricks.py:119-152) with the Hybrid synchrotron model
+ * (python/blackhole_sim/synchrotron.py:240-325): per cell the local plasma frame
+ * of coefficient_bricks.py:110-116 (n_e = rho * rho_cgs_per_code / (mu_e m_p),
+ * B = |b_con[1:4]| * b_gauss_per_code, EVPA = atan2(b^3, b^2), Theta_e floored
+ * at 1e-8, no line-of-sight pitch), then the thermal and power-law
+ * components' 11 coefficients, summed, rotated by the EVPA and written in
+ * COEFF_NAMES order with the brick dtype's nan_to_num.  FP64 throughout. */
+typedef struct bhn_synchrotron_model {
+    double nu_hz;
+    double rho_cgs_per_code, b_gauss_per_code, mean_molecular_weight_per_electron;  /* PhysicalScaling */
+    int32_t thermal, nonthermal;                   /* which components the model sums (Hybrid: both) */
+    int32_t thermal_gamma_n, thermal_pitch_n;      /* ThermalSynchrotronCoefficients: 192, 16 */
+    double thermal_rotation_scale, thermal_conversion_scale;                 /* 1, 1 */
+    int32_t nonthermal_gamma_n, nonthermal_pitch_n;                          /* 224, 16 */
+    double nonthermal_p, nonthermal_gamma_min, nonthermal_gamma_max;         /* 3.5, 10, 1e5 */
+    double nonthermal_fraction, nonthermal_absorption_scale, nonthermal_faraday_scale;  /* 0.02, 1, 0.15 */
+} bhn_synchrotron_model;
+
+/* rho, theta_e: [cells] float64 (device); b_con: [cells][4] float64 (device);
+ * coeffs: [cells][11] of coeff_bytes (4 or 8) each (device).  Gamma grids take
+ * 2..4096 nodes, pitch averages 1..64. */
+int bhn_brick_precompute(const double *rho, const double *theta_e, const double *b_con, int64_t cells,
+                         const bhn_synchrotron_model *model, void *coeffs, int32_t coeff_bytes, void *stream);
 
 /* CUDA-graph form of bhn_render_launch: captures the queue reset and the
  * persistent launch once; bhn_graph_launch replays it on `stream`. */

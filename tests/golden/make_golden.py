@@ -6,7 +6,7 @@ Run in a container where the reference project is mounted (read-only):
 
 Every output value in the fixtures is computed by the reference's own Python
 functions (python/blackhole_sim/native_kernels.py, kerr.py,
-accelerated_renderer.py).  The ray-loop fixtures compose those functions the
+accelerated_renderer.py, coefficient_bricks.py with synchrotron.py).  The ray-loop fixtures compose those functions the
 way the brick renderer does (accelerated_renderer.py:129-150), with the RK2
 midpoint step of native/cuda/kerr_stokes_kernel.cu:13 in place of rk4_step and
 the variable step h = clamp(0.02 r, 1e-3, 1).  Inputs are seeded and stored
@@ -271,14 +271,70 @@ def ray_fixtures(kerr, acc, bricks_mod) -> dict[str, np.ndarray]:
     return out
 
 
+def precompute_snapshot(seed: int = 7):
+    """Seeded small GRMHD-like snapshot: 5 x 4 x 3 cells over the reference's
+    usable range (Thetae 0 .. 200 including the 1e-8 floor and cold cells,
+    fields of either sign and a zero-field cell)."""
+    rng = np.random.default_rng(seed)
+    a = 0.9375
+    r_plus = 1.0 + math.sqrt(1.0 - a * a)
+    r = np.geomspace(1.05 * r_plus, 40.0, 5)
+    theta = (np.arange(4) + 0.5) * math.pi / 4.0
+    phi = np.linspace(0.0, 2.0 * math.pi, 3, endpoint=False)
+    shape = (r.size, theta.size, phi.size)
+    rho = np.exp(-((r[:, None, None] - 8.0) ** 2) / 8.0 - 4.0 * np.cos(theta)[None, :, None] ** 2) \
+        * np.exp(rng.normal(0.0, 0.3, shape))
+    theta_e = np.exp(rng.uniform(np.log(0.05), np.log(200.0), shape))
+    theta_e[0, 0, 0] = 0.0            # floored to 1e-8 by the reference
+    theta_e[0, 1, 0] = 1.0e-3         # cold: no thermal emission at 230 GHz
+    b_con = rng.normal(0.0, 1.0, shape + (4,))
+    b_con[1, 1, 1, 1:] = 0.0          # zero field: every coefficient 0
+    u_con = np.zeros(shape + (4,))
+    u_con[..., 0] = 1.0
+    pressure = rho * theta_e
+    return dict(r=r, theta=theta, phi=phi, rho=rho, theta_e=theta_e, pressure=pressure, b_con=b_con, u_con=u_con,
+                spin_a=a)
+
+
+def precompute_fixtures(grmhd, calibration, cb, synchrotron) -> dict[str, np.ndarray]:
+    """precompute_coefficient_bricks (coefficient_bricks.py:119-152) with the
+    Hybrid model (synchrotron.py) on the seeded snapshot, in float64 and float32,
+    plus the reference's F/G kernel table (synchrotron.py:196-201)."""
+    snap = precompute_snapshot()
+    scaling = calibration.PhysicalScaling(mass_bh_g=8.54e39, distance_cm=2.57e22, rho_cgs_per_code=3.0e-18,
+                                          b_gauss_per_code=25.0)
+    g = grmhd.GRMHDSnapshot(**snap)
+    out = {f"in_{k}": np.asarray(v) for k, v in snap.items()}
+    out["in_rho_cgs_per_code"] = np.asarray(scaling.rho_cgs_per_code)
+    out["in_b_gauss_per_code"] = np.asarray(scaling.b_gauss_per_code)
+    out["in_mu_e"] = np.asarray(scaling.mean_molecular_weight_per_electron)
+    for nu in (230e9, 86e9):
+        t0 = time.time()
+        b64 = cb.precompute_coefficient_bricks(g, scaling, nu_hz=nu, dtype="float64")
+        b32 = cb.precompute_coefficient_bricks(g, scaling, nu_hz=nu, dtype="float32")
+        tag = f"{int(nu / 1e9)}"
+        out[f"coeffs64_{tag}"] = np.asarray(b64.coeffs)
+        out[f"coeffs32_{tag}"] = np.asarray(b32.coeffs)
+        print(f"  precompute nu={nu:.3g}: {time.time() - t0:.1f}s", flush=True)
+    b2 = cb.precompute_coefficient_bricks(g, scaling, nu_hz=230e9, dtype="float64", stride=2)
+    out["coeffs64_230_stride2"] = np.asarray(b2.coeffs)
+    xs, F, G = synchrotron._synchrotron_kernel_table()
+    out["table_xs"], out["table_F"], out["table_G"] = xs, F, G
+    mu, w = np.polynomial.legendre.leggauss(16)
+    out["leggauss16_mu"], out["leggauss16_w"] = mu, w
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/python")
-    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray")
+    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
     from blackhole_sim import accelerated_renderer as acc, benchmark as bench, kerr, native_kernels as nk
+    from blackhole_sim import calibration, grmhd, synchrotron
+    from blackhole_sim import coefficient_bricks as cb
     from blackhole_native import bricks as bricks_mod
 
     only = set(filter(None, args.only.split(",")))
@@ -291,6 +347,9 @@ def main() -> None:
     if not only or "ray" in only:
         np.savez_compressed(HERE / "ray_loop.npz", **ray_fixtures(kerr, acc, bricks_mod))
         print("wrote ray_loop.npz")
+    if not only or "precompute" in only:
+        np.savez_compressed(HERE / "brick_precompute.npz", **precompute_fixtures(grmhd, calibration, cb, synchrotron))
+        print("wrote brick_precompute.npz")
 
 
 if __name__ == "__main__":

@@ -74,6 +74,27 @@ def test_struct_layouts_match_ctypes(tmp_path):
     assert got == want
 
 
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
+def test_parameter_struct_layouts_match_ctypes(tmp_path):
+    """bhn_adapt_params and bhn_synchrotron_model against their ctypes mirrors."""
+    from blackhole_native import learned, synchrotron
+
+    src = tmp_path / "sizes2.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "blackhole_native.h"\n'
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(bhn_adapt_params),"
+        " offsetof(bhn_adapt_params, fallback), offsetof(bhn_adapt_params, seed), sizeof(bhn_synchrotron_model),"
+        " offsetof(bhn_synchrotron_model, nonthermal_gamma_n), offsetof(bhn_synchrotron_model, nonthermal_faraday_scale));"
+        " return 0;}\n")
+    exe = tmp_path / "sizes2"
+    subprocess.run(["gcc", "-I", str(REPO / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    A, M = learned.AdaptStruct, synchrotron.ModelStruct
+    want = [ctypes.sizeof(A), A.fallback.offset, A.seed.offset, ctypes.sizeof(M), M.nonthermal_gamma_n.offset,
+            M.nonthermal_faraday_scale.offset]
+    assert got == want
+
+
 def test_compute_calls_fail_loudly_without_gpu():
     import torch
 

@@ -1,8 +1,8 @@
 """GPU parity of the fused ray kernel against the oracle.
 
 * FP64 kernel: the oracle's arithmetic on the GPU -> image rel L1 <= 1e-9 and
-  identical step counts / statuses (the north-star bar for FP64-matched runs
-  is rel L1 <= 1e-5).
+  identical step counts / statuses (the bar for FP64-matched runs is rel L1
+  <= 1e-5).
 * FP32 kernel (the product): Stokes I rel L1 <= 1e-3 and flux-weighted
   polarization-fraction error <= 1e-2 against the FP64 oracle.
 * Cell location: bit-exact with numpy.searchsorted(side="right") - 1.
@@ -262,6 +262,6 @@ def test_zero_steps_and_no_brick_hits(golden_brick):
     b, db = golden_brick
     z = bn.render(db, bn.View(8, 6, max_steps=0), precision="fp32", ray_outputs=True)
     assert torch.count_nonzero(z.image()) == 0 and z.stats().status["max_steps"] == 48
-    # BASELINE config 1 as stated: no ray reaches r = 40 M in 64 steps -> exact zeros
+    # the 32x18, 64-step CPU case: no ray reaches r = 40 M in 64 steps -> exact zeros
     c1 = bn.render(db, bn.View(32, 18, max_steps=64), precision="fp32", ray_outputs=True)
     assert torch.count_nonzero(c1.image()) == 0 and c1.stats().brick_steps == 0
