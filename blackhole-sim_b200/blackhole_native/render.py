@@ -181,6 +181,14 @@ class DeviceBrick:
     def cells(self) -> int:
         return self.nr * self.nt * self.np
 
+    def twin(self) -> "DeviceBrick":
+        """A brick on the same grids (shared tables) with its own record
+        buffers, initialised to this brick's values."""
+        obj = DeviceBrick.__new__(DeviceBrick)
+        obj.__dict__.update({k: v for k, v in self.__dict__.items() if k != "_records"})
+        obj._records = {p: r.clone() for p, r in self._records.items()}
+        return obj
+
     def reload(self, coeffs: torch.Tensor | np.ndarray, staging: torch.Tensor | None = None,
                check_finite: bool = True) -> torch.Tensor:
         """Replace the brick values (same grids) from host memory: one host->device
@@ -380,6 +388,73 @@ class Renderer:
 
     def result(self) -> RenderResult:
         return RenderResult(self.views, self.out, self.offsets, self.stats_buf, self.steps, self.status, self.h_drift)
+
+
+class PipelinedRenderer:
+    """Renders a sequence of bricks on the same grids (successive snapshots of
+    a simulation, say) for fixed views, overlapping data movement with the
+    kernel: while brick k renders, brick k + 1 is copied from pinned host memory
+    on a copy stream and image k - 1 is copied back on a third stream.  Two
+    record buffers, two raw staging buffers and two compiled launches
+    alternate; events order every buffer's reuse.  Host bricks must be pinned
+    (``tensor.pin_memory()``) for the copies to overlap."""
+
+    def __init__(self, brick: DeviceBrick, views: Sequence[View], *, config: RenderConfig | None = None,
+                 precision: str = "fp32"):
+        self.precision = precision
+        self.bricks = [brick, brick.twin()]
+        self.renderers = [Renderer(b, views, config=config, precision=precision) for b in self.bricks]
+        for r in self.renderers:
+            r.capture()
+        dev_ = brick.device
+        self.copy_stream = torch.cuda.Stream(dev_)
+        self.d2h_stream = torch.cuda.Stream(dev_)
+        self.staging: list[torch.Tensor | None] = [None, None]
+        ev = lambda: [torch.cuda.Event(), torch.cuda.Event()]  # noqa: E731
+        self.copied, self.packed, self.rendered, self.fetched = ev(), ev(), ev(), ev()
+        self.out_shape = self.renderers[0].out.shape
+        self.out_dtype = self.renderers[0].out.dtype
+
+    def run(self, host_bricks: Sequence[torch.Tensor], host_outs: Sequence[torch.Tensor]) -> None:
+        """Render host_bricks[k] (raw [nr][nt][np][11] values, pinned) into
+        host_outs[k % len(host_outs)] (pinned, the renderer's output shape).
+        Returns once all work is queued; synchronise the current stream (which
+        waits for the copy streams) before reading the last images."""
+        compute = torch.cuda.current_stream(self.bricks[0].device)
+        cells = self.bricks[0].cells * 11
+        # buffers of an earlier run are free once the work queued before this call is done
+        self.copy_stream.wait_stream(compute)
+        self.d2h_stream.wait_stream(compute)
+        for k, hb in enumerate(host_bricks):
+            s = k % 2
+            src = hb.reshape(-1)
+            if src.numel() != cells:
+                raise ValueError(f"brick {k} must contain exactly r*theta*phi*11 values; expected {cells}")
+            if self.staging[s] is None or self.staging[s].dtype != src.dtype:
+                self.staging[s] = torch.empty(cells, dtype=src.dtype, device=self.bricks[0].device)
+            with torch.cuda.stream(self.copy_stream):
+                if k >= 2:  # staging[s] is free once brick k - 2 has been packed
+                    self.copy_stream.wait_event(self.packed[s])
+                self.staging[s].copy_(src, non_blocking=True)
+                self.copied[s].record(self.copy_stream)
+            compute.wait_event(self.copied[s])
+            self.bricks[s]._pack(self.staging[s], self.precision, check_finite=False)
+            self.packed[s].record(compute)
+            if k >= 2:  # the output buffer is free once image k - 2 has been fetched
+                compute.wait_event(self.fetched[s])
+            self.renderers[s].graph_launch()
+            self.rendered[s].record(compute)
+            dst = host_outs[k % len(host_outs)]
+            with torch.cuda.stream(self.d2h_stream):
+                self.d2h_stream.wait_event(self.rendered[s])
+                dst.copy_(self.renderers[s].out, non_blocking=True)
+                self.fetched[s].record(self.d2h_stream)
+        compute.wait_stream(self.copy_stream)
+        compute.wait_stream(self.d2h_stream)
+
+    def release(self) -> None:
+        for r in self.renderers:
+            r.release_graph()
 
 
 def render(brick: DeviceBrick, views: Sequence[View] | View, *, precision: str = "fp32",
