@@ -102,6 +102,18 @@ def stokes_rk2_brick(coeffs, ds_cm, initial):
     coeffs: flat cells*11 values; initial: 4 (broadcast) or 4*cells values.
     Returns the flat cells*4 stepped Stokes values.
     """
+    return _stokes_brick(coeffs, ds_cm, initial, "bhn_stokes_rk2_brick")
+
+
+def stokes_exact_brick(coeffs, ds_cm, initial):
+    """One exact constant-coefficient Stokes step per coefficient cell: the
+    augmented matrix exponential of polarized_transfer.stokes_step_exact
+    (python/blackhole_sim/polarized_transfer.py:51-70), batched over cells,
+    with the inputs and validation of stokes_rk2_brick."""
+    return _stokes_brick(coeffs, ds_cm, initial, "bhn_stokes_exact_brick")
+
+
+def _stokes_brick(coeffs, ds_cm, initial, entry):
     ds = _ds(ds_cm)
     if _any_cuda(coeffs, initial):
         device = dev.require_cuda()
@@ -117,8 +129,8 @@ def stokes_rk2_brick(coeffs, ds_cm, initial):
         if dev.check_values_device(ini, False)[0]:
             raise ValueError("initial must contain only finite values")
         out = torch.empty(cells * STOKES_COMPONENTS, dtype=torch.float64, device=device)
-        _lib.check(_lib.lib().bhn_stokes_rk2_brick(dev.ptr(c), cells, ds, dev.ptr(ini), ini.numel(), dev.ptr(out),
-                                                   dev.stream_ptr()))
+        _lib.check(getattr(_lib.lib(), entry)(dev.ptr(c), cells, ds, dev.ptr(ini), ini.numel(), dev.ptr(out),
+                                              dev.stream_ptr()))
         return out
     c = dev.host_f64(coeffs)
     if c.size == 0 or c.size % COEFFS_PER_CELL:
@@ -134,8 +146,8 @@ def stokes_rk2_brick(coeffs, ds_cm, initial):
     device = dev.require_cuda()
     dc, di = dev.to_device(c, device), dev.to_device(ini, device)
     out = torch.empty(cells * STOKES_COMPONENTS, dtype=torch.float64, device=device)
-    _lib.check(_lib.lib().bhn_stokes_rk2_brick(dev.ptr(dc), cells, ds, dev.ptr(di), ini.size, dev.ptr(out),
-                                               dev.stream_ptr()))
+    _lib.check(getattr(_lib.lib(), entry)(dev.ptr(dc), cells, ds, dev.ptr(di), ini.size, dev.ptr(out),
+                                          dev.stream_ptr()))
     return out.cpu().numpy().tolist()
 
 

@@ -13,6 +13,7 @@
 #include <string>
 
 #include "bhn_internal.cuh"
+#include "bhn_transfer.cuh"
 
 namespace bhn {
 
@@ -136,6 +137,20 @@ __global__ void stokes_rk2_brick_kernel(const double *__restrict__ coeffs, int64
         const double *s0 = initial + (broadcast ? 0 : 4 * i);
         double s[4] = {s0[0], s0[1], s0[2], s0[3]};
         stokes_step_rk2_exact(s, c, ds);
+        reinterpret_cast<double2 *>(out + 4 * i)[0] = make_double2(s[0], s[1]);
+        reinterpret_cast<double2 *>(out + 4 * i)[1] = make_double2(s[2], s[3]);
+    }
+}
+
+__global__ void stokes_exact_brick_kernel(const double *__restrict__ coeffs, int64_t cells, double ds,
+                                          const double *__restrict__ initial, int broadcast, double *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cells; i += (int64_t)gridDim.x * blockDim.x) {
+        double c[11];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) c[k] = coeffs[11 * i + k];
+        const double *s0 = initial + (broadcast ? 0 : 4 * i);
+        double s[4] = {s0[0], s0[1], s0[2], s0[3]};
+        stokes_step_exact(s, c, ds);
         reinterpret_cast<double2 *>(out + 4 * i)[0] = make_double2(s[0], s[1]);
         reinterpret_cast<double2 *>(out + 4 * i)[1] = make_double2(s[2], s[3]);
     }
@@ -376,6 +391,18 @@ int bhn_stokes_rk2_brick(const double *coeffs, int64_t cells, double ds_cm, cons
     stokes_rk2_brick_kernel<<<grid_for(cells, 256), 256, 0, as_stream(stream)>>>(coeffs, cells, ds_cm, initial,
                                                                                  initial_len == 4, out);
     BHN_LAUNCH_CHECK("stokes_rk2_brick_kernel");
+    return BHN_OK;
+}
+
+int bhn_stokes_exact_brick(const double *coeffs, int64_t cells, double ds_cm, const double *initial,
+                           int64_t initial_len, double *out, void *stream) {
+    if (!std::isfinite(ds_cm) || ds_cm < 0.0) return fail(BHN_ERR_VALUE, "ds_cm must be finite and non-negative");
+    if (cells <= 0) return fail(BHN_ERR_VALUE, "coeffs must contain one or more flat 11-coefficient cells");
+    if (initial_len != 4 && initial_len != 4 * cells)
+        return fail(BHN_ERR_VALUE, "initial must contain either 4 values or 4 values per coefficient cell");
+    stokes_exact_brick_kernel<<<grid_for(cells, 128), 128, 0, as_stream(stream)>>>(coeffs, cells, ds_cm, initial,
+                                                                                   initial_len == 4, out);
+    BHN_LAUNCH_CHECK("stokes_exact_brick_kernel");
     return BHN_OK;
 }
 

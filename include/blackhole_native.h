@@ -70,6 +70,15 @@ int bhn_fp32_peak_probe(float *scratch, int32_t iters, int32_t blocks_per_sm, in
 int bhn_stokes_rk2_brick(const double *coeffs, int64_t cells, double ds_cm, const double *initial,
                          int64_t initial_len, double *out, void *stream);
 
+/* The exact constant-coefficient Stokes step of
+ * python/blackhole_sim/polarized_transfer.py:51-70 (stokes_step_exact: the
+ * 5x5 augmented exponential exp([[-K, j], [0, 0]] ds) applied to [S; 1]) for
+ * every cell, with the input contract of bhn_stokes_rk2_brick.  The reference
+ * evaluates it one step at a time through scipy.linalg.expm; here by scaling
+ * and squaring with a truncated Taylor series in FP64. */
+int bhn_stokes_exact_brick(const double *coeffs, int64_t cells, double ds_cm, const double *initial,
+                           int64_t initial_len, double *out, void *stream);
+
 /* Replaces sample_brick_trilinear (native/core/src/lib.rs:281-306).  coeffs:
  * nr*nt*np*11 in [r][theta][phi][11] order, points: n*3 (r, theta, phi),
  * out: n*11 with NaN rows outside the nonperiodic r/theta domain. */

@@ -6,7 +6,8 @@ Run in a container where the reference project is mounted (read-only):
 
 Every output value in the fixtures is computed by the reference's own Python
 functions (python/blackhole_sim/native_kernels.py, kerr.py,
-accelerated_renderer.py, coefficient_bricks.py with synchrotron.py).  The ray-loop fixtures compose those functions the
+accelerated_renderer.py, coefficient_bricks.py with synchrotron.py,
+polarized_transfer.py).  The ray-loop fixtures compose those functions the
 way the brick renderer does (accelerated_renderer.py:129-150), with the RK2
 midpoint step of native/cuda/kerr_stokes_kernel.cu:13 in place of rk4_step and
 the variable step h = clamp(0.02 r, 1e-3, 1).  Inputs are seeded and stored
@@ -325,15 +326,45 @@ def precompute_fixtures(grmhd, calibration, cb, synchrotron) -> dict[str, np.nda
     return out
 
 
+def exact_step_fixtures(pt, synchrotron) -> dict[str, np.ndarray]:
+    """polarized_transfer.stokes_step_exact (polarized_transfer.py:51-70) on
+    seeded coefficient sets and step lengths, including pure emission, pure
+    absorption, pure Faraday rotation / conversion, optically thick steps and
+    a zero step."""
+    rng = np.random.default_rng(20260203)
+    cases = []
+    for _ in range(40):
+        c = rng.normal(0.0, 1.0, 11)
+        c[4] = abs(c[4]) + 0.5 * np.linalg.norm(c[5:8])     # alpha_I >= |alpha_pol|: a physical absorber
+        cases.append(c)
+    special = np.zeros((6, 11))
+    special[0, :4] = [1.0, 0.3, -0.2, 0.05]                # emission only
+    special[1, 4] = 2.0                                    # absorption only
+    special[2, 8:11] = [3.0, 0.0, 0.0]                     # Faraday rotation only
+    special[3, 8:11] = [0.0, 1.5, -0.7]                    # Faraday conversion only
+    special[4] = [1, 0.5, 0.2, 0.1, 3.0, 1.0, -0.5, 0.3, 5.0, -2.0, 1.0]
+    special[5] = [2e-20, 1e-21, 0, 0, 1e-18, 0, 0, 0, 3e-18, 1e-19, 0]
+    coeffs = np.vstack([np.array(cases), special])
+    ds_list = np.array([0.0, 1.0e-3, 0.1, 1.0, 7.5, 60.0])
+    rng2 = np.random.default_rng(5)
+    initial = rng2.normal(0.0, 1.0, (coeffs.shape[0], 4))
+    out = np.zeros((ds_list.size, coeffs.shape[0], 4))
+    for i, ds in enumerate(ds_list):
+        for k, c in enumerate(coeffs):
+            out[i, k] = pt.stokes_step_exact(initial[k], synchrotron.PolarizedCoefficients(*c), float(ds))
+    return {"exact_coeffs": coeffs, "exact_initial": initial, "exact_ds": ds_list, "exact_out": out}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/python")
-    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute")
+    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
     from blackhole_sim import accelerated_renderer as acc, benchmark as bench, kerr, native_kernels as nk
     from blackhole_sim import calibration, grmhd, synchrotron
+    from blackhole_sim import polarized_transfer as pt
     from blackhole_sim import coefficient_bricks as cb
     from blackhole_native import bricks as bricks_mod
 
@@ -350,6 +381,9 @@ def main() -> None:
     if not only or "precompute" in only:
         np.savez_compressed(HERE / "brick_precompute.npz", **precompute_fixtures(grmhd, calibration, cb, synchrotron))
         print("wrote brick_precompute.npz")
+    if not only or "exact" in only:
+        np.savez_compressed(HERE / "exact_step.npz", **exact_step_fixtures(pt, synchrotron))
+        print("wrote exact_step.npz")
 
 
 if __name__ == "__main__":
