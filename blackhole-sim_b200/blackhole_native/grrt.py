@@ -1,0 +1,173 @@
+"""Physical polarized GRRT through a GRMHD snapshot on the GPU.
+
+Drop-in for ``polarized_renderer.render_stokes_image`` (python/blackhole_sim/
+polarized_renderer.py:31-70): per pixel the camera ray, a fixed-step RK4 Kerr
+geodesic (kerr.py:337-384) and ``integrate_polarized_kerr_grrt``
+(polarized_transfer.py:83-145) -- snapshot sampled at every segment's
+midpoint, invariant redshift, synchrotron coefficients of the plasma frame at
+the emitted frequency, exact or RK2 Stokes steps -- all in one FP64 CUDA
+kernel (``bhn_grrt_render``, one warp per ray).
+
+The configuration, camera, snapshot and scaling arguments are duck-typed: the
+reference's own ``PolarizedRenderConfig`` / ``LocalCamera`` /
+``GRMHDSnapshot`` / ``PhysicalScaling`` objects work, and so do this module's
+mirrors of the first two.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _device as dev
+from . import _lib
+from .synchrotron import HybridSynchrotronCoefficients, ModelStruct, model_struct
+
+G_CGS = 6.67430e-8       # calibration.py:19
+C_CGS = 2.99792458e10    # calibration.py:18
+
+
+@dataclass(frozen=True)
+class LocalCamera:
+    """kerr.py:155-185 (theta, phi in radians)."""
+
+    r: float = 50.0
+    theta: float = math.radians(60.0)
+    phi: float = 0.0
+    fov_y_degrees: float = 35.0
+    roll_degrees: float = 0.0
+
+    @classmethod
+    def from_degrees(cls, r: float = 50.0, inclination_degrees: float = 60.0, phi_degrees: float = 0.0,
+                     fov_y_degrees: float = 35.0, roll_degrees: float = 0.0) -> "LocalCamera":
+        return cls(r=r, theta=math.radians(inclination_degrees), phi=math.radians(phi_degrees),
+                   fov_y_degrees=fov_y_degrees, roll_degrees=roll_degrees)
+
+
+@dataclass(frozen=True)
+class PolarizedTransferConfig:
+    """polarized_transfer.py:22-28."""
+
+    observing_frequency_hz: float = 230.0e9
+    affine_to_length_cm: float | None = None
+    max_optical_depth: float = 30.0
+    min_redshift: float = 1.0e-8
+    use_exact_matrix_step: bool = True
+
+
+@dataclass(frozen=True)
+class PolarizedRenderConfig:
+    """polarized_renderer.py:21-30 (``workers`` and ``tone_map`` are accepted and unused: the GPU
+    renders every pixel in one launch and returns the raw Stokes image)."""
+
+    width: int = 160
+    height: int = 90
+    camera: LocalCamera = field(default_factory=lambda: LocalCamera.from_degrees(r=55.0, inclination_degrees=65.0,
+                                                                                  fov_y_degrees=32.0))
+    step: float = 0.06
+    max_steps: int = 5000
+    escape_radius: float = 220.0
+    workers: int = 1
+    transfer: PolarizedTransferConfig = field(default_factory=lambda: PolarizedTransferConfig(use_exact_matrix_step=False))
+    tone_map: bool = True
+
+
+class GrrtConfigStruct(ctypes.Structure):
+    """``bhn_grrt_config``."""
+
+    _fields_ = [
+        ("step", ctypes.c_double),
+        ("escape_radius", ctypes.c_double),
+        ("nu_hz", ctypes.c_double),
+        ("length_cm", ctypes.c_double),
+        ("max_optical_depth", ctypes.c_double),
+        ("min_redshift", ctypes.c_double),
+        ("flux_scale", ctypes.c_double),
+        ("max_steps", ctypes.c_int32),
+        ("exact_step", ctypes.c_int32),
+    ]
+
+
+DIAGNOSTICS = ("optical_depth", "emitting_steps", "valid_steps", "faraday_depth_abs", "redshift_min", "redshift_max",
+               "steps", "status")
+
+
+def _declare() -> ctypes.CDLL:
+    L = _lib.lib()
+    fn = L.bhn_grrt_render
+    vp, i32 = ctypes.c_void_p, ctypes.c_int32
+    fn.argtypes = [vp, vp, i32, vp, i32, vp, i32, ctypes.POINTER(_lib.ViewStruct), ctypes.POINTER(ModelStruct),
+                   ctypes.POINTER(GrrtConfigStruct), vp, ctypes.c_int64, vp, vp, vp]
+    fn.restype = ctypes.c_int
+    return L
+
+
+def snapshot_fields(snapshot) -> np.ndarray:
+    """[nr][nt][np][11] float64: rho, Theta_e, pressure, b^mu, u^mu (grmhd.py:55-68)."""
+    shape = (np.asarray(snapshot.r).size, np.asarray(snapshot.theta).size, np.asarray(snapshot.phi).size)
+    parts = [np.asarray(snapshot.rho, dtype=np.float64)[..., None], np.asarray(snapshot.theta_e, dtype=np.float64)[..., None],
+             np.asarray(snapshot.pressure, dtype=np.float64)[..., None], np.asarray(snapshot.b_con, dtype=np.float64),
+             np.asarray(snapshot.u_con, dtype=np.float64)]
+    f = np.ascontiguousarray(np.concatenate(parts, axis=-1))
+    if f.shape != shape + (11,):
+        raise ValueError(f"snapshot fields must have shape {shape} (b_con, u_con {shape + (4,)})")
+    return f
+
+
+def _length_cm(transfer, scaling) -> float:
+    if getattr(transfer, "affine_to_length_cm", None) is not None:
+        return float(transfer.affine_to_length_cm)
+    rg = getattr(scaling, "rg_cm", None)
+    if rg is None:
+        rg = G_CGS * float(scaling.mass_bh_g) / (C_CGS * C_CGS)  # calibration.py:107-109
+    return float(rg)
+
+
+def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diagnostics: bool = False,
+                               device: torch.device | None = None):
+    """(H, W, 4) float64 Stokes image on the device (and (H, W, 8) diagnostics,
+    columns ``DIAGNOSTICS``, when asked)."""
+    L = _declare()
+    device = device or dev.require_cuda()
+    for name in ("r", "theta", "phi"):
+        g = np.asarray(getattr(snapshot, name), dtype=np.float64)
+        if g.ndim != 1 or g.size < 2 or np.any(np.diff(g) <= 0.0):
+            raise ValueError(f"{name} grid must be a strictly increasing 1-D array")
+    grids = [torch.as_tensor(np.ascontiguousarray(np.asarray(getattr(snapshot, n), dtype=np.float64)), device=device)
+             for n in ("r", "theta", "phi")]
+    fields = torch.as_tensor(snapshot_fields(snapshot), device=device)
+    cam = cfg.camera
+    v = _lib.ViewStruct()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = float(snapshot.spin_a), float(cam.r), float(cam.theta), float(cam.phi)
+    v.fov_y_deg, v.roll_deg = float(cam.fov_y_degrees), float(getattr(cam, "roll_degrees", 0.0))
+    v.h_scale, v.h_min, v.h_max = 0.02, 1e-3, 1.0  # unused by the fixed-step loop
+    v.escape_radius, v.affine_to_length_cm, v.max_optical_depth = float(cfg.escape_radius), 1.0, 30.0
+    v.width, v.height, v.x0, v.y0, v.crop_w, v.crop_h = int(cfg.width), int(cfg.height), 0, 0, int(cfg.width), int(cfg.height)
+    v.max_steps, v.flags, v.out_offset = int(cfg.max_steps), 0, 0
+    if v.width < 1 or v.height < 1:
+        raise ValueError("image width and height must be positive")
+    t = cfg.transfer
+    c = GrrtConfigStruct()
+    c.step, c.escape_radius, c.nu_hz = float(cfg.step), float(cfg.escape_radius), float(t.observing_frequency_hz)
+    c.length_cm, c.max_optical_depth, c.min_redshift = _length_cm(t, scaling), float(t.max_optical_depth), float(t.min_redshift)
+    c.flux_scale = float(getattr(scaling, "flux_scale_jy", 1.0))
+    c.max_steps, c.exact_step = int(cfg.max_steps), int(bool(t.use_exact_matrix_step))
+    m = model_struct(coeff_model or HybridSynchrotronCoefficients(), t.observing_frequency_hz, scaling)
+    nbytes = int(L.bhn_render_scratch_bytes(1))
+    scratch = torch.zeros(nbytes // 8 + 64, dtype=torch.float64, device=device)
+    sp = (dev.ptr(scratch) + 255) & ~255
+    out = torch.empty((v.height, v.width, 4), dtype=torch.float64, device=device)
+    diag = torch.empty((v.height, v.width, 8), dtype=torch.float64, device=device) if diagnostics else None
+    _lib.check(L.bhn_grrt_render(dev.ptr(fields), dev.ptr(grids[0]), grids[0].numel(), dev.ptr(grids[1]),
+                                 grids[1].numel(), dev.ptr(grids[2]), grids[2].numel(), ctypes.byref(v), ctypes.byref(m),
+                                 ctypes.byref(c), sp, nbytes, dev.ptr(out), dev.ptr(diag), dev.stream_ptr()))
+    return (out, diag) if diagnostics else out
+
+
+def render_stokes_image(cfg, snapshot, scaling, progress: bool = False, *, coeff_model=None):
+    """polarized_renderer.py:56-70 on the GPU: the (H, W, 4) float64 Stokes image."""
+    return render_stokes_image_device(cfg, snapshot, scaling, coeff_model=coeff_model).cpu().numpy()

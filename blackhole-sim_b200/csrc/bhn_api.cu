@@ -14,6 +14,7 @@
 
 #include "bhn_internal.cuh"
 #include "bhn_transfer.cuh"
+#include "bhn_exact.cuh"
 
 namespace bhn {
 
@@ -43,89 +44,7 @@ int sm_count_current_device() {
     return cached[dev];
 }
 
-// ------------------------------------------------------------ exact helpers
-__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
-
-// lib.rs:37-59 / native_kernels.py:213-222, evaluated left to right.
-__device__ __forceinline__ void stokes_rhs_exact(const double s[4], const double c[11], double o[4]) {
-    o[0] = sub(c[0], add(add(add(mul(c[4], s[0]), mul(c[5], s[1])), mul(c[6], s[2])), mul(c[7], s[3])));
-    o[1] = sub(c[1], sub(add(add(mul(c[5], s[0]), mul(c[4], s[1])), mul(c[8], s[2])), mul(c[10], s[3])));
-    o[2] = sub(c[2], add(add(sub(mul(c[6], s[0]), mul(c[8], s[1])), mul(c[4], s[2])), mul(c[9], s[3])));
-    o[3] = sub(c[3], add(sub(add(mul(c[7], s[0]), mul(c[10], s[1])), mul(c[9], s[2])), mul(c[4], s[3])));
-}
-
-// lib.rs:210-225
-__device__ __forceinline__ void stokes_step_rk2_exact(double s[4], const double c[11], double ds) {
-    double k1[4], mid[4], k2[4];
-    double hds = mul(0.5, ds);
-    stokes_rhs_exact(s, c, k1);
-    for (int i = 0; i < 4; ++i) mid[i] = add(s[i], mul(hds, k1[i]));
-    stokes_rhs_exact(mid, c, k2);
-    for (int i = 0; i < 4; ++i) s[i] = add(s[i], mul(ds, k2[i]));
-}
-
-// lib.rs:75-87 / native_kernels.py:137-146
-__device__ __forceinline__ bool bracket_linear_exact(const double *g, int n, double x, int &i0, double &w) {
-    if (x < g[0] || x > g[n - 1]) return false;
-    if (x == g[n - 1]) {
-        i0 = n - 2;
-        w = 1.0;
-        return true;
-    }
-    int lo = search_right(g, 0, n, x) - 1;
-    lo = max(0, min(lo, n - 2));
-    double den = sub(g[lo + 1], g[lo]);
-    if (den < 1.0e-300) den = 1.0e-300;
-    i0 = lo;
-    w = sub(x, g[lo]) / den;
-    return true;
-}
-
-// lib.rs:93-106 / native_kernels.py:149-161
-__device__ __forceinline__ void bracket_phi_exact(const double *g, int n, double phi, int &i0, int &i1, double &w) {
-    double p = wrap_phi(phi, g[0]);
-    int lo = search_right(g, 0, n, p) - 1;
-    if (lo < 0) lo = n - 1;
-    if (lo >= n) lo = n - 1;
-    int hi_i = (lo + 1) % n;
-    double hi = hi_i > lo ? g[hi_i] : add(g[0], kTwoPi);
-    double pp = p >= g[lo] ? p : add(p, kTwoPi);
-    double den = sub(hi, g[lo]);
-    if (den < 1.0e-300) den = 1.0e-300;
-    i0 = lo;
-    i1 = hi_i;
-    w = sub(pp, g[lo]) / den;
-}
-
-// lib.rs:171-208 / native_kernels.py:164-186
-__device__ __forceinline__ bool sample_one_exact(const double *__restrict__ coeffs, const double *rg, int nr,
-                                                 const double *tg, int nt, const double *pg, int np, double r,
-                                                 double th, double ph, double out[11]) {
-    int r0, t0, p0, p1;
-    double wr, wt, wp;
-    if (!bracket_linear_exact(rg, nr, r, r0, wr) || !bracket_linear_exact(tg, nt, th, t0, wt)) return false;
-    bracket_phi_exact(pg, np, ph, p0, p1, wp);
-    const int r1 = r0 + 1, t1 = t0 + 1;
-    auto off = [&](int ir, int it, int ip) { return ((((int64_t)ir * nt + it) * np) + ip) * 11; };
-    const double *c000 = coeffs + off(r0, t0, p0), *c001 = coeffs + off(r0, t0, p1);
-    const double *c010 = coeffs + off(r0, t1, p0), *c011 = coeffs + off(r0, t1, p1);
-    const double *c100 = coeffs + off(r1, t0, p0), *c101 = coeffs + off(r1, t0, p1);
-    const double *c110 = coeffs + off(r1, t1, p0), *c111 = coeffs + off(r1, t1, p1);
-    const double owp = sub(1.0, wp), owt = sub(1.0, wt), owr = sub(1.0, wr);
-#pragma unroll
-    for (int c = 0; c < 11; ++c) {
-        double c00 = add(mul(owp, c000[c]), mul(wp, c001[c]));
-        double c01 = add(mul(owp, c010[c]), mul(wp, c011[c]));
-        double c10 = add(mul(owp, c100[c]), mul(wp, c101[c]));
-        double c11 = add(mul(owp, c110[c]), mul(wp, c111[c]));
-        double cc0 = add(mul(owt, c00), mul(wt, c01));
-        double cc1 = add(mul(owt, c10), mul(wt, c11));
-        out[c] = add(mul(owr, cc0), mul(wr, cc1));
-    }
-    return true;
-}
+// exact helpers: bhn_exact.cuh
 
 // ------------------------------------------------------------------- kernels
 __global__ void stokes_rk2_brick_kernel(const double *__restrict__ coeffs, int64_t cells, double ds,

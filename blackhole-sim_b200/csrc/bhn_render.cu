@@ -25,8 +25,10 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "bhn_internal.cuh"
 
@@ -1229,3 +1231,4 @@ int bhn_graph_destroy(bhn_graph *graph) {
 
 }  // extern "C"
 #include "bhn_learned.cuh"
+#include "bhn_grrt.cuh"

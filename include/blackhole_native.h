@@ -321,6 +321,31 @@ typedef struct bhn_synchrotron_model {
 int bhn_brick_precompute(const double *rho, const double *theta_e, const double *b_con, int64_t cells,
                          const bhn_synchrotron_model *model, void *coeffs, int32_t coeff_bytes, void *stream);
 
+/* ---- physical polarized GRRT through a GRMHD snapshot --------------------------
+ * Replaces polarized_renderer.render_stokes_image (python/blackhole_sim/
+ * polarized_renderer.py:31-70): per pixel of one view, the camera ray
+ * (kerr.py:188-233), a fixed-step RK4 geodesic (kerr.py:306-313, 337-384) and
+ * integrate_polarized_kerr_grrt (polarized_transfer.py:83-145) with the
+ * synchrotron model of bhn_brick_precompute, in FP64.  fields:
+ * [nr][nt][np][11] float64 = rho, Theta_e, pressure, b^mu (4), u^mu (4) of the
+ * snapshot (grmhd.py:55-121); out: [rays][4] Stokes of the view's crop in row
+ * order (at view->out_offset); diag (optional): [rays][8] = optical depth,
+ * emitting segments, valid segments, Faraday depth, min / max redshift,
+ * steps traced, BHN_RAY_* status.  scratch: bhn_render_scratch_bytes(1). */
+typedef struct bhn_grrt_config {
+    double step;                 /* affine RK4 step (PolarizedRenderConfig.step) */
+    double escape_radius;
+    double nu_hz;                /* observing frequency */
+    double length_cm;            /* affine-to-length scale (the scaling's r_g when not given) */
+    double max_optical_depth, min_redshift, flux_scale;
+    int32_t max_steps;
+    int32_t exact_step;          /* 1: stokes_step_exact, 0: RK2 (PolarizedTransferConfig.use_exact_matrix_step) */
+} bhn_grrt_config;
+int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, const double *theta_grid, int32_t nt,
+                    const double *phi_grid, int32_t np, const bhn_view *view, const bhn_synchrotron_model *model,
+                    const bhn_grrt_config *cfg, void *scratch, int64_t scratch_bytes, double *out, double *diag,
+                    void *stream);
+
 /* CUDA-graph form of bhn_render_launch: captures the queue reset and the
  * persistent launch once; bhn_graph_launch replays it on `stream`. */
 typedef struct bhn_graph bhn_graph;

@@ -307,6 +307,58 @@ void bho_rk2_step(const double y[6], double h, double a, double pt, double pphi,
     out[2] = bho_safe_theta(out[2]);
 }
 
+static int all_finite6(const double y[6]);
+
+/* kerr.py:306-313: classical RK4, theta clamped. */
+void bho_rk4_step(const double y[6], double h, double a, double pt, double pphi, double out[6]) {
+    double k1[6], k2[6], k3[6], k4[6], tmp[6];
+    double hh = 0.5 * h;
+    bho_geodesic_rhs(y, a, pt, pphi, k1);
+    for (int i = 0; i < 6; ++i) tmp[i] = y[i] + hh * k1[i];
+    bho_geodesic_rhs(tmp, a, pt, pphi, k2);
+    for (int i = 0; i < 6; ++i) tmp[i] = y[i] + hh * k2[i];
+    bho_geodesic_rhs(tmp, a, pt, pphi, k3);
+    for (int i = 0; i < 6; ++i) tmp[i] = y[i] + h * k3[i];
+    bho_geodesic_rhs(tmp, a, pt, pphi, k4);
+    double h6 = h / 6.0;
+    for (int i = 0; i < 6; ++i) out[i] = y[i] + h6 * (((k1[i] + 2.0 * k2[i]) + 2.0 * k3[i]) + k4[i]);
+    out[2] = bho_safe_theta(out[2]);
+}
+
+/* kerr.py:337-384 trace_kerr_null_geodesic with store_stride 1: writes the
+ * stored states (at most max_steps + 1 rows of 6) and returns their count;
+ * *status: 0 max_steps, 1 captured, 2 escaped, 3 invalid. */
+int64_t bho_trace_rk4(const double y0[6], double pt, double pphi, double a, double h, int32_t max_steps,
+                      double escape_radius, double *states, int32_t *status) {
+    double y[6], yn[6];
+    memcpy(y, y0, sizeof y);
+    memcpy(states, y, sizeof y);
+    int64_t n = 1;
+    double r_capture = bho_horizon_radius(a) * (1.0 + 2.0e-4);
+    double prev_r = y[1];
+    *status = BHO_STATUS_MAX_STEPS;
+    for (int32_t i = 1; i <= max_steps; ++i) {
+        bho_rk4_step(y, h, a, pt, pphi, yn);
+        if (!all_finite6(yn)) {
+            *status = BHO_STATUS_INVALID;
+            break;
+        }
+        memcpy(y, yn, sizeof y);
+        memcpy(states + 6 * n, y, sizeof y);
+        ++n;
+        if (y[1] <= r_capture) {
+            *status = BHO_STATUS_CAPTURED;
+            break;
+        }
+        if (y[1] > escape_radius && y[1] > prev_r) {
+            *status = BHO_STATUS_ESCAPED;
+            break;
+        }
+        prev_r = y[1];
+    }
+    return n;
+}
+
 /* kerr.py:188-233 camera_ray_initial_state with kerr.py:124-152 zamo_tetrad. */
 int bho_camera_ray(const bho_view *v, double ndc_x, double ndc_y, double aspect, double y0[6], double *pt,
                    double *pphi) {

@@ -73,6 +73,9 @@ void bho_geodesic_rhs(const double y[6], double a, double pt, double pphi, doubl
 /* RK2 midpoint step (native/cuda/kerr_stokes_kernel.cu:13 form) on the analytic
  * RHS, theta clamped like kerr.py:312. */
 void bho_rk2_step(const double y[6], double h, double a, double pt, double pphi, double out[6]);
+void bho_rk4_step(const double y[6], double h, double a, double pt, double pphi, double out[6]);
+int64_t bho_trace_rk4(const double y0[6], double pt, double pphi, double a, double h, int32_t max_steps,
+                      double escape_radius, double *states, int32_t *status);
 
 /* One camera view: kerr.py:155-233 LocalCamera + accelerated_renderer.py:36-46. */
 typedef struct bho_view {

@@ -74,6 +74,9 @@ def lib() -> ctypes.CDLL:
         _lib.bho_sample_brick_valid_mask.argtypes = [vp, i64, vp, i64, vp, i64, vp]
         _lib.bho_geodesic_rhs.argtypes = [vp, d, d, d, vp]
         _lib.bho_rk2_step.argtypes = [vp, d, d, d, d, vp]
+        _lib.bho_rk4_step.argtypes = [vp, d, d, d, d, vp]
+        _lib.bho_trace_rk4.argtypes = [vp, d, d, d, d, ctypes.c_int32, d, vp, ctypes.POINTER(ctypes.c_int32)]
+        _lib.bho_trace_rk4.restype = i64
         _lib.bho_hamiltonian.argtypes = [vp, d, d, d]
         _lib.bho_hamiltonian.restype = d
         _lib.bho_camera_ray.argtypes = [ctypes.POINTER(View), d, d, d, vp, ctypes.POINTER(d), ctypes.POINTER(d)]
@@ -141,6 +144,24 @@ def rk2_step(y, h, a, pt, pphi) -> np.ndarray:
     out = np.empty(6)
     lib().bho_rk2_step(_p(yy), h, a, pt, pphi, _p(out))
     return out
+
+
+def trace_rk4(y0, pt, pphi, a, h, max_steps, escape_radius):
+    """kerr.py:337-384 (store_stride 1): (states (n, 6), status 0..3)."""
+    states = np.empty((int(max_steps) + 1, 6))
+    st = ctypes.c_int32()
+    n = lib().bho_trace_rk4(_p(_f64(y0)), pt, pphi, a, h, int(max_steps), escape_radius, _p(states), ctypes.byref(st))
+    return states[:n].copy(), int(st.value)
+
+
+def camera_ray(view, ndc_x, ndc_y, aspect):
+    """kerr.py:188-233: (y0 (6,), p_t, p_phi)."""
+    y0 = np.zeros(6)
+    pt, pphi = ctypes.c_double(), ctypes.c_double()
+    rc = lib().bho_camera_ray(ctypes.byref(view), ndc_x, ndc_y, aspect, _p(y0), ctypes.byref(pt), ctypes.byref(pphi))
+    if rc != 0:
+        raise ValueError("invalid camera")
+    return y0, pt.value, pphi.value
 
 
 def hamiltonian(y, a, pt, pphi) -> float:

@@ -130,8 +130,8 @@ def _rotated(c, chi):
                      rv, rq * co - ru * si, rq * si + ru * co])
 
 
-def thermal(n_e, theta_e, b_gauss, evpa, nu_hz, m=THERMAL):
-    """synchrotron.py:189-196, 248-275 with cos_pitch_to_los = 0 (so b_parallel = 0)."""
+def thermal(n_e, theta_e, b_gauss, evpa, nu_hz, m=THERMAL, cos_los=0.0):
+    """synchrotron.py:189-196, 248-275 (brick frames have cos_pitch_to_los = 0)."""
     if n_e <= 0.0 or b_gauss <= 0.0 or nu_hz <= 0.0:
         return np.zeros(11)
     gmax = max(10.0, 1.0 + 45.0 * theta_e)
@@ -144,15 +144,19 @@ def thermal(n_e, theta_e, b_gauss, evpa, nu_hz, m=THERMAL):
     Bnu = planck_nu(nu_hz, theta_e)
     alphaI = jI / max(Bnu, 1.0e-300)
     alphaQ0 = jQ0 / max(Bnu, 1.0e-300)
-    rhoV = 0.0  # b_parallel = b cos_pitch_to_los = 0 (coefficient_bricks.py:116)
+    b_perp = abs(b_gauss) * math.sqrt(max(0.0, 1.0 - cos_los ** 2))  # synchrotron.py:37-43
+    b_par = b_gauss * cos_los
+    rel_supp = max(1.0 / (theta_e * theta_e + 1.0), 1.0e-8)
+    rhoV = m["faraday_rotation_scale"] * (E_CHARGE_ESU ** 3 / (math.pi * M_ELECTRON_CGS ** 2 * C_CGS ** 2))
+    rhoV *= n_e * b_par / max(nu_hz * nu_hz, 1.0e-300) * rel_supp
     rhoQ = m["faraday_conversion_scale"] * (E_CHARGE_ESU ** 4 / (4.0 * math.pi ** 2 * M_ELECTRON_CGS ** 3 * C_CGS ** 3))
-    rhoQ *= n_e * b_gauss ** 2 / max(nu_hz ** 3, 1.0e-300) * max(theta_e, 1.0e-8)
+    rhoQ *= n_e * b_perp ** 2 / max(nu_hz ** 3, 1.0e-300) * max(theta_e, 1.0e-8)
     c = [max(jI, 0.0), max(jQ0, 0.0), 0.0, 0.0, max(alphaI, 0.0), max(alphaQ0, 0.0), 0.0, 0.0, rhoV, rhoQ, 0.0]
     return _rotated(c, evpa)
 
 
-def nonthermal(n_e, theta_e, b_gauss, evpa, nu_hz, m=NONTHERMAL):
-    """synchrotron.py:199-204, 290-311 with cos_pitch_to_los = 0."""
+def nonthermal(n_e, theta_e, b_gauss, evpa, nu_hz, m=NONTHERMAL, cos_los=0.0):
+    """synchrotron.py:199-204, 290-311."""
     if n_e <= 0.0 or b_gauss <= 0.0 or nu_hz <= 0.0 or m["nonthermal_fraction"] <= 0.0:
         return np.zeros(11)
     p, gmin, gmax = m["p"], m["gamma_min"], m["gamma_max"]
@@ -163,15 +167,18 @@ def nonthermal(n_e, theta_e, b_gauss, evpa, nu_hz, m=NONTHERMAL):
     f = f / max(np.trapezoid(f, gamma), 1.0e-300)
     n_s = n_e * m["nonthermal_fraction"]
     jI, jQ0 = integrated_j(n_s, b_gauss, nu_hz, gamma, f, m["pitch_nodes"])
-    char_gamma = max(gmin, math.sqrt(max(nu_hz / max(4.2e6 * b_gauss, 1.0e-300), 1.0)))
+    b_perp = abs(b_gauss) * math.sqrt(max(0.0, 1.0 - cos_los ** 2))
+    b_par = b_gauss * cos_los
+    char_gamma = max(gmin, math.sqrt(max(nu_hz / max(4.2e6 * b_perp, 1.0e-300), 1.0)))
     energy = char_gamma * M_ELECTRON_CGS * C_CGS * C_CGS
     alphaI = m["absorption_scale"] * jI / max(energy * nu_hz * nu_hz / (C_CGS * C_CGS), 1.0e-300)
     pol_frac = min((p + 1.0) / (p + 7.0 / 3.0), 0.85)
     jQ0 = min(jQ0, pol_frac * jI)
     alphaQ0 = min(alphaI * pol_frac, alphaI)
-    rhoV = 0.0
+    rhoV = m["faraday_scale"] * (E_CHARGE_ESU ** 3 / (math.pi * M_ELECTRON_CGS ** 2 * C_CGS ** 2))
+    rhoV *= n_s * b_par / max(nu_hz * nu_hz, 1.0e-300) / max(gmin ** 2, 1.0)
     rhoQ = m["faraday_scale"] * (E_CHARGE_ESU ** 4 / (4.0 * math.pi ** 2 * M_ELECTRON_CGS ** 3 * C_CGS ** 3))
-    rhoQ *= n_s * b_gauss ** 2 / max(nu_hz ** 3, 1.0e-300) * math.log(max(gmax / gmin, 1.0))
+    rhoQ *= n_s * b_perp ** 2 / max(nu_hz ** 3, 1.0e-300) * math.log(max(gmax / gmin, 1.0))
     c = [max(jI, 0.0), max(jQ0, 0.0), 0.0, 0.0, max(alphaI, 0.0), max(alphaQ0, 0.0), 0.0, 0.0, rhoV, rhoQ, 0.0]
     return _rotated(c, evpa)
 

@@ -7,7 +7,7 @@ Run in a container where the reference project is mounted (read-only):
 Every output value in the fixtures is computed by the reference's own Python
 functions (python/blackhole_sim/native_kernels.py, kerr.py,
 accelerated_renderer.py, coefficient_bricks.py with synchrotron.py,
-polarized_transfer.py).  The ray-loop fixtures compose those functions the
+polarized_transfer.py, polarized_renderer.py).  The ray-loop fixtures compose those functions the
 way the brick renderer does (accelerated_renderer.py:129-150), with the RK2
 midpoint step of native/cuda/kerr_stokes_kernel.cu:13 in place of rk4_step and
 the variable step h = clamp(0.02 r, 1e-3, 1).  Inputs are seeded and stored
@@ -355,16 +355,61 @@ def exact_step_fixtures(pt, synchrotron) -> dict[str, np.ndarray]:
     return {"exact_coeffs": coeffs, "exact_initial": initial, "exact_ds": ds_list, "exact_out": out}
 
 
+def grrt_snapshot(seed: int = 11):
+    """Seeded GRMHD-like snapshot on a 12 x 8 x 6 grid for the physical
+    renderer: torus density, Thetae 1..60, random fields, slowly rotating
+    flow u = (1, 0, 0, Omega(r))."""
+    rng = np.random.default_rng(seed)
+    a = 0.9375
+    r_plus = 1.0 + math.sqrt(1.0 - a * a)
+    r = np.geomspace(1.05 * r_plus, 40.0, 12)
+    theta = (np.arange(8) + 0.5) * math.pi / 8.0
+    phi = np.linspace(0.0, 2.0 * math.pi, 6, endpoint=False)
+    shape = (r.size, theta.size, phi.size)
+    rho = np.exp(-((r[:, None, None] - 8.0) ** 2) / 8.0 - 4.0 * np.cos(theta)[None, :, None] ** 2) \
+        * np.exp(rng.normal(0.0, 0.2, shape))
+    theta_e = np.exp(rng.uniform(0.0, np.log(60.0), shape))
+    b_con = rng.normal(0.0, 1.0, shape + (4,))
+    u_con = np.zeros(shape + (4,))
+    u_con[..., 0] = 1.0
+    u_con[..., 3] = (0.5 * r[:, None, None] ** -1.5) * np.ones(shape)
+    return dict(r=r, theta=theta, phi=phi, rho=rho, theta_e=theta_e, pressure=rho * theta_e, b_con=b_con,
+                u_con=u_con, spin_a=a)
+
+
+def grrt_fixtures(grmhd, calibration, kerr, pr) -> dict[str, np.ndarray]:
+    """polarized_renderer.render_stokes_image (polarized_renderer.py:31-70) on a
+    4 x 3 image of the seeded snapshot, RK2 and exact Stokes steps."""
+    snap = grrt_snapshot()
+    g = grmhd.GRMHDSnapshot(**snap)
+    scaling = calibration.PhysicalScaling(mass_bh_g=8.54e39, distance_cm=2.57e22, rho_cgs_per_code=3.0e-18,
+                                          b_gauss_per_code=25.0)
+    out = {f"in_{k}": np.asarray(v) for k, v in snap.items()}
+    out["in_rho_cgs_per_code"] = np.asarray(scaling.rho_cgs_per_code)
+    out["in_b_gauss_per_code"] = np.asarray(scaling.b_gauss_per_code)
+    out["in_rg_cm"] = np.asarray(scaling.rg_cm)
+    cam = kerr.LocalCamera.from_degrees(r=30.0, inclination_degrees=65.0, fov_y_degrees=32.0)
+    out["cam"] = np.array([cam.r, cam.theta, cam.phi, cam.fov_y_degrees, cam.roll_degrees])
+    for exact in (False, True):
+        cfg = pr.PolarizedRenderConfig(width=4, height=3, camera=cam, step=0.1, max_steps=900, escape_radius=220.0,
+                                       workers=1, transfer=pr.PolarizedTransferConfig(use_exact_matrix_step=exact))
+        t0 = time.time()
+        out[f"stokes_{'exact' if exact else 'rk2'}"] = pr.render_stokes_image(cfg, g, scaling)
+        print(f"  grrt exact={exact}: {time.time() - t0:.1f}s", flush=True)
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/python")
-    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact")
+    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
     from blackhole_sim import accelerated_renderer as acc, benchmark as bench, kerr, native_kernels as nk
     from blackhole_sim import calibration, grmhd, synchrotron
     from blackhole_sim import polarized_transfer as pt
+    from blackhole_sim import polarized_renderer as pr
     from blackhole_sim import coefficient_bricks as cb
     from blackhole_native import bricks as bricks_mod
 
@@ -384,6 +429,9 @@ def main() -> None:
     if not only or "exact" in only:
         np.savez_compressed(HERE / "exact_step.npz", **exact_step_fixtures(pt, synchrotron))
         print("wrote exact_step.npz")
+    if not only or "grrt" in only:
+        np.savez_compressed(HERE / "grrt.npz", **grrt_fixtures(grmhd, calibration, kerr, pr))
+        print("wrote grrt.npz")
 
 
 if __name__ == "__main__":
