@@ -51,7 +51,7 @@ __device__ __forceinline__ void rk4_state(const double y[5], double h, double a,
     yn[4] = y[4] + h6 * (((k1.pth + 2.0 * k2.pth) + 2.0 * k3.pth) + k4.pth);
 }
 
-__global__ void __launch_bounds__(128) grrt_kernel(const __grid_constant__ GrrtParams P) {
+__global__ void __launch_bounds__(128, 4) grrt_kernel(const __grid_constant__ GrrtParams P) {
     __shared__ synch::TableSmem T;
     synch::load_table(T, P.M);
     __syncthreads();
