@@ -57,6 +57,7 @@ class BrickGrid:
     phi: np.ndarray
     coeffs: np.ndarray
     spin_a: float = 0.0
+    nu_hz: float = 230.0e9          # observing frequency the coefficients were computed at
 
     def __post_init__(self) -> None:
         for name in ("r", "theta", "phi"):
@@ -78,14 +79,47 @@ class BrickGrid:
         return int(self.r.size * self.theta.size * self.phi.size)
 
     def save_npz(self, path) -> None:
-        """Same keys as coefficient_bricks.py:57-66 (minus the frequency)."""
+        """The file layout of CoefficientBrickGrid.save_npz (coefficient_bricks.py:57-70):
+        r, theta, phi, coeffs, coeff_names, nu_hz, spin_a, dtype_name; the
+        reference's load_npz reads it (it keeps grids as float32)."""
+        from pathlib import Path
+
+        Path(path).parent.mkdir(parents=True, exist_ok=True)
         np.savez_compressed(path, r=self.r, theta=self.theta, phi=self.phi, coeffs=self.coeffs,
-                            coeff_names=np.array(COEFF_NAMES), spin_a=np.array(self.spin_a))
+                            coeff_names=np.array(COEFF_NAMES), nu_hz=np.array(self.nu_hz),
+                            spin_a=np.array(self.spin_a), dtype_name=np.array(self.coeffs.dtype.name))
 
     @classmethod
     def load_npz(cls, path) -> "BrickGrid":
+        """Reads this class's files and the reference's (coefficient_bricks.py:72-75);
+        channel order is checked when the file names its channels."""
         with np.load(path, allow_pickle=False) as z:
-            return cls(z["r"], z["theta"], z["phi"], z["coeffs"], float(z["spin_a"]) if "spin_a" in z else 0.0)
+            if "coeff_names" in z and tuple(str(n) for n in z["coeff_names"]) != COEFF_NAMES:
+                raise ValueError(f"brick channels {tuple(z['coeff_names'])} differ from {COEFF_NAMES}")
+            return cls(z["r"], z["theta"], z["phi"], z["coeffs"], float(z["spin_a"]) if "spin_a" in z else 0.0,
+                       float(z["nu_hz"]) if "nu_hz" in z else 230.0e9)
+
+    def save_hdf5(self, path) -> None:
+        """The HDF5 schema of CoefficientBrickGrid.save_hdf5 (coefficient_bricks.py:77-93):
+        attributes schema / nu_hz / spin_a / dtype_name, gzip+shuffle datasets
+        r, theta, phi, coeffs (chunked) and coeff_names.  Needs h5py."""
+        try:
+            import h5py  # type: ignore
+        except ImportError as exc:
+            raise RuntimeError("h5py is required for HDF5 coefficient bricks") from exc
+        from pathlib import Path
+
+        p = Path(path)
+        p.parent.mkdir(parents=True, exist_ok=True)
+        with h5py.File(p, "w") as f:
+            f.attrs["schema"] = "blackhole_sim.coefficient_bricks.v1"
+            f.attrs["nu_hz"] = self.nu_hz
+            f.attrs["spin_a"] = self.spin_a
+            f.attrs["dtype_name"] = self.coeffs.dtype.name
+            for name in ("r", "theta", "phi"):
+                f.create_dataset(name, data=getattr(self, name), compression="gzip", shuffle=True)
+            f.create_dataset("coeffs", data=self.coeffs, compression="gzip", shuffle=True, chunks=True)
+            f.create_dataset("coeff_names", data=np.asarray(COEFF_NAMES, dtype="S"))
 
 
 def torus_grids(nr: int, ntheta: int, nphi: int, spin_a: float, dtype=np.float32):

@@ -149,6 +149,12 @@ class DeviceBrick:
             self._pack(coeffs, p)
 
     @classmethod
+    def from_npz(cls, path, device: torch.device | None = None, precisions: Sequence[str] = ("fp32",)) -> "DeviceBrick":
+        """A brick file (this package's or the reference's CoefficientBrickGrid
+        npz) loaded straight into HBM."""
+        return cls(BrickGrid.load_npz(path), device=device, precisions=precisions)
+
+    @classmethod
     def from_device_coeffs(cls, r, theta, phi, coeffs: torch.Tensor, spin_a: float = 0.0,
                            precisions: Sequence[str] = ("fp32",)) -> "DeviceBrick":
         """A brick whose [nr][nt][np][11] values already live on the device

@@ -399,10 +399,20 @@ def grrt_fixtures(grmhd, calibration, kerr, pr) -> dict[str, np.ndarray]:
     return out
 
 
+def brick_npz_fixture(cb, path) -> None:
+    """A small brick written by CoefficientBrickGrid.save_npz (coefficient_bricks.py:57-70)."""
+    rng = np.random.default_rng(9)
+    r = np.geomspace(1.5, 40.0, 4)
+    theta = (np.arange(3) + 0.5) * math.pi / 3.0
+    phi = np.linspace(0.0, 2.0 * math.pi, 5, endpoint=False)
+    coeffs = rng.uniform(0.0, 1.0, (4, 3, 5, 11)).astype(np.float32)
+    cb.CoefficientBrickGrid(r, theta, phi, coeffs, 86e9, 0.5, "float32").save_npz(path)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/python")
-    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt")
+    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
@@ -429,6 +439,9 @@ def main() -> None:
     if not only or "exact" in only:
         np.savez_compressed(HERE / "exact_step.npz", **exact_step_fixtures(pt, synchrotron))
         print("wrote exact_step.npz")
+    if not only or "bricknpz" in only:
+        brick_npz_fixture(cb, HERE / "reference_brick.npz")
+        print("wrote reference_brick.npz")
     if not only or "grrt" in only:
         np.savez_compressed(HERE / "grrt.npz", **grrt_fixtures(grmhd, calibration, kerr, pr))
         print("wrote grrt.npz")
