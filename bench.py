@@ -12,6 +12,11 @@ divided by the device time of the timed steps, summed over all GPUs.
 
 --impl reference times the reference algorithm's CPU restatement (the float64
 oracle, OpenMP over every host core) on a bounded sample of the same workload.
+
+Other workloads (--workload): views (256 uneven views in one launch),
+precompute (coefficient bricks from a 256 x 128 x 256 seeded snapshot, cells/s)
+and grrt (the physical polarized renderer's default 160 x 90 image, pixels/s);
+their lines carry an FP64 exp() roofline measured in the same run.
 For N > 1 the job runs as torchrun ranks, one full image per rank (replicas:
 rays are independent and the path has no exchange step).
 """
@@ -168,11 +173,11 @@ def load_peaks() -> dict:
     return {"hbm_gbs": FALLBACK_HBM_GBS, "source": "fallback"}
 
 
-def profiled_traffic() -> float | None:
-    """DRAM bytes per launch of the render kernel from the committed ncu summary."""
-    if not PROFILE_SUMMARY.exists():
+def profiled_traffic(summary: Path = PROFILE_SUMMARY) -> float | None:
+    """DRAM bytes per launch of a kernel from its committed ncu summary."""
+    if not summary.exists():
         return None
-    for line in PROFILE_SUMMARY.read_text().splitlines():
+    for line in summary.read_text().splitlines():
         if line.strip().startswith("traffic_bytes_per_launch:"):
             try:
                 return float(line.split(":", 1)[1].strip().split()[0])
@@ -470,6 +475,328 @@ def bench_views(args) -> dict | None:
     return line if rank == 0 else None
 
 
+# ------------------------------------------------------------------ synchrotron workloads
+PRECOMPUTE = dict(nr=256, ntheta=128, nphi=256, spin_a=0.9375, seed=5, nu_hz=230e9)
+PRECOMPUTE_PROFILE = REPO / "profiles" / "precompute_kernel_snapshot_2M_cells.md"
+PRECOMPUTE_PROFILE_CELLS = 64 * 128 * 256   # the captured case; its traffic scales with the cells
+GRRT_SNAPSHOT = dict(nr=64, ntheta=32, nphi=64, spin_a=0.9375, seed=0)
+# calibration.PhysicalScaling of a 4.3e6 solar-mass hole at 8.3 kpc with code units rho 3e-18 g/cm^3, B 25 G
+SCALING = dict(mass_bh_g=8.54e39, distance_cm=2.57e22, rho_cgs_per_code=3.0e-18, b_gauss_per_code=25.0)
+
+
+def fp64_peaks(device, stream) -> dict:
+    """FP64 FMA TFLOP/s and double exp() evaluations/s of this GPU (bhn_fp64_peak_probe)."""
+    import ctypes
+
+    import torch
+
+    from blackhole_native import _lib
+
+    L = _lib.lib()
+    probe = torch.empty(1 << 20, dtype=torch.float64, device=device)
+    out = {}
+    for mode, iters, key in ((0, 2048, "fma_tflops"), (1, 512, "exp_per_s")):
+        ops = ctypes.c_int64()
+        for _ in range(2):
+            _lib.check(L.bhn_fp64_peak_probe(probe.data_ptr(), iters, 8, mode, ctypes.byref(ops), stream.cuda_stream))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(L.bhn_fp64_peak_probe(probe.data_ptr(), iters, 8, mode, ctypes.byref(ops), stream.cuda_stream))
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        rate = ops.value / (e0.elapsed_time(e1) * 1e-3)
+        out[key] = rate / 1e12 if mode == 0 else rate
+    return out
+
+
+def exps_per_evaluation(model_struct) -> int:
+    """Double exp() calls of the kernel-table lookups in one coefficient
+    evaluation: F and G at every (Lorentz-factor node, pitch node) pair of
+    each component."""
+    m = model_struct
+    n = 0
+    if m.thermal:
+        n += m.thermal_gamma_n * m.thermal_pitch_n
+    if m.nonthermal:
+        n += m.nonthermal_gamma_n * m.nonthermal_pitch_n
+    return 2 * n
+
+
+def exp_roofline(evals: float, seconds: float, peaks: dict, per_eval: int, kernel: str) -> dict:
+    achieved = evals * per_eval / seconds
+    return {"bound": "fp64-exp", "achieved": round(achieved / 1e9, 2), "peak": round(peaks["exp_per_s"] / 1e9, 2),
+            "unit": "Gexp/s", "frac": round(achieved / peaks["exp_per_s"], 4), "traffic": None,
+            "peak_source": "measured in this run (bhn_fp64_peak_probe, 8 chains of x <- exp(-x) per thread)",
+            "kernel": kernel, "exp_per_unit": per_eval,
+            "fp64_fma_tflops_measured": round(peaks["fma_tflops"], 2)}
+
+
+def timed_launches(fn, k: int, stream, device) -> list[float]:
+    import torch
+
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(k + 1)]
+    torch.cuda.synchronize(device)
+    evs[0].record(stream)
+    for i in range(k):
+        fn()
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize(device)
+    return [evs[i].elapsed_time(evs[i + 1]) for i in range(k)]
+
+
+def bench_precompute(args) -> dict | None:
+    """Coefficient-brick precompute (coefficient_bricks.py:119-152, Hybrid
+    model): one step = every cell of a 256 x 128 x 256 seeded snapshot to an
+    [nr][nt][np][11] float32 brick."""
+    import ctypes
+
+    import torch
+
+    from blackhole_native import _device as dev
+    from blackhole_native import grrt, synchrotron as syn
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    init_dist(world, "nccl")
+    stream = torch.cuda.current_stream(device)
+    P = dict(PRECOMPUTE)
+    if args.side:  # fewer r shells of the same snapshot layout (profiling runs)
+        P["nr"] = args.side
+    snap = grrt.seeded_snapshot(P["nr"], P["ntheta"], P["nphi"], P["spin_a"], P["seed"])
+    scaling = grrt.PhysicalScaling(**SCALING)
+    cells = P["nr"] * P["ntheta"] * P["nphi"]
+    L = syn._declare()
+    m = syn.model_struct(syn.HybridSynchrotronCoefficients(), P["nu_hz"], scaling)
+    d_rho = torch.from_numpy(np.ascontiguousarray(snap.rho)).to(device)
+    d_te = torch.from_numpy(np.ascontiguousarray(snap.theta_e)).to(device)
+    d_b = torch.from_numpy(np.ascontiguousarray(snap.b_con)).to(device)
+    out = torch.empty((P["nr"], P["ntheta"], P["nphi"], 11), dtype=torch.float32, device=device)
+
+    def launch():
+        _lib_check(L.bhn_brick_precompute(dev.ptr(d_rho), dev.ptr(d_te), dev.ptr(d_b), cells, ctypes.byref(m),
+                                          dev.ptr(out), 4, stream.cuda_stream))
+
+    peaks = fp64_peaks(device, stream)
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize(device)
+    assert bool(torch.isfinite(out).all()), "non-finite coefficients"
+    clocks = ClockSampler(_uuid(device)).start()
+    time.sleep(0.3)
+    barrier(world)
+    per = timed_launches(launch, args.steps, stream, device)
+    barrier(world)
+    clk = clocks.stop()
+    t_max = max_over_ranks(sum(per), world, device)
+    value = sum_over_ranks(cells * args.steps, world, device) / (t_max * 1e-3)
+
+    e2e = None
+    if not args.no_e2e:  # public API with host arrays: fields up, brick back to host
+        ke = max(1, min(args.steps, 3))
+        ref = out.cpu().numpy()
+        syn.precompute_coefficient_bricks(snap, scaling, P["nu_hz"])
+        barrier(world)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        a0.record(stream)
+        for _ in range(ke):
+            brick = syn.precompute_coefficient_bricks(snap, scaling, P["nu_hz"])
+        a1.record(stream)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        te = max_over_ranks(a0.elapsed_time(a1), world, device)
+        assert np.array_equal(brick.coeffs, ref), "public-API brick differs from the device launch"
+        e2e = {"value": sum_over_ranks(cells * ke, world, device) / (te * 1e-3), "unit": "cells/s",
+               "h2d_bytes_per_step": int(cells * 6 * 8), "d2h_bytes_per_step": int(cells * 11 * 4),
+               "ms_per_step": te / ke, "api": "precompute_coefficient_bricks"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = precompute_cpu_baseline(snap, scaling, args.cpu_seconds)
+    per_mean = statistics.mean(per)
+    line = {
+        "metric": "cells/s", "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"coefficient-brick precompute, Hybrid synchrotron model at 230 GHz: "
+                               f"{P['nr']}x{P['ntheta']}x{P['nphi']} seeded GRMHD-like snapshot -> float32 "
+                               "[nr][nt][np][11] brick",
+                   "cells_per_step": cells, "l2": f"inputs larger than L2 ({cells * 48 / 1e6:.0f} MB of float64 fields)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
+        "roofline": dict(exp_roofline(cells, per_mean * 1e-3, peaks, exps_per_evaluation(m), "precompute_kernel"),
+                         traffic=_scaled_traffic(PRECOMPUTE_PROFILE, cells / PRECOMPUTE_PROFILE_CELLS)),
+        "cpu_baseline": cpu,
+        "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
+    }
+    if world > 1:
+        import torch.distributed as td
+
+        td.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def precompute_cpu_baseline(snap, scaling, target_s: float) -> dict:
+    """The float64 oracle (per-cell numpy loop, one core) on a run of cells."""
+    sys.path.insert(0, str(REPO))
+    from oracle import synchrotron as S
+
+    rho = snap.rho.reshape(-1)
+    te = snap.theta_e.reshape(-1)
+    b = snap.b_con.reshape(-1, 4)
+    start = rho.size // 2
+
+    def run(n):
+        sl = slice(start, start + n)
+        t0 = time.perf_counter()
+        S.precompute(rho[sl].reshape(1, 1, n), te[sl].reshape(1, 1, n), b[sl].reshape(1, 1, n, 4),
+                     PRECOMPUTE["nu_hz"], scaling.rho_cgs_per_code, scaling.b_gauss_per_code)
+        return time.perf_counter() - t0
+
+    dt = run(4)
+    n = max(4, min(20000, int(4 * max(target_s, 0.5) / max(dt, 1e-4))))
+    dt = run(n)
+    return {"value": n / dt, "unit": "cells/s", "cores": 1, "kind": "port",
+            "sample": f"float64 oracle (oracle/synchrotron.py, numpy per cell, one core): {n} cells of the same "
+                      f"snapshot in {dt:.2f} s"}
+
+
+def bench_grrt(args) -> dict | None:
+    """Physical polarized GRRT (polarized_renderer.render_stokes_image): one
+    step = the reference's default 160 x 90 image (camera r = 55 M, i = 65 deg,
+    FOV 32 deg, RK4 step 0.06, 5000 steps, RK2 Stokes steps) of a seeded
+    64 x 32 x 64 snapshot."""
+    import torch
+
+    from blackhole_native import grrt
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    init_dist(world, "nccl")
+    stream = torch.cuda.current_stream(device)
+    G = GRRT_SNAPSHOT
+    snap = grrt.seeded_snapshot(G["nr"], G["ntheta"], G["nphi"], G["spin_a"], G["seed"])
+    scaling = grrt.PhysicalScaling(**SCALING)
+    cfg = grrt.PolarizedRenderConfig()
+    if args.side:  # a smaller image of the same scene (profiling runs)
+        cfg = grrt.PolarizedRenderConfig(width=args.side, height=max(1, round(args.side * 9 / 16)))
+    ds = grrt.DeviceSnapshot(snap, device)
+    pixels = cfg.width * cfg.height
+    img, diag = grrt.render_stokes_image_device(cfg, ds, scaling, diagnostics=True)
+    torch.cuda.synchronize(device)
+    d = diag.cpu().numpy()
+    segments, steps = float(d[..., 1].sum()), float(d[..., 6].sum())
+    out = torch.empty_like(img)
+    peaks = fp64_peaks(device, stream)
+    for _ in range(args.warmup):
+        grrt.render_stokes_image_device(cfg, ds, scaling, out=out)
+    clocks = ClockSampler(_uuid(device)).start()
+    time.sleep(0.3)
+    barrier(world)
+    per = timed_launches(lambda: grrt.render_stokes_image_device(cfg, ds, scaling, out=out), args.steps, stream,
+                         device)
+    barrier(world)
+    clk = clocks.stop()
+    assert torch.equal(out, img), "images differ between launches"
+    t_max = max_over_ranks(sum(per), world, device)
+    value = sum_over_ranks(pixels * args.steps, world, device) / (t_max * 1e-3)
+
+    e2e = None
+    if not args.no_e2e:  # public API: host snapshot in, host image out
+        ke = max(1, min(args.steps, 3))
+        barrier(world)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        a0.record(stream)
+        for _ in range(ke):
+            host = grrt.render_stokes_image(cfg, snap, scaling)
+        a1.record(stream)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        te = max_over_ranks(a0.elapsed_time(a1), world, device)
+        assert np.array_equal(host, img.cpu().numpy()), "public-API image differs from the device launch"
+        e2e = {"value": sum_over_ranks(pixels * ke, world, device) / (te * 1e-3), "unit": "pixels/s",
+               "h2d_bytes_per_step": ds.upload_bytes, "d2h_bytes_per_step": int(pixels * 4 * 8),
+               "ms_per_step": te / ke, "api": "render_stokes_image"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = grrt_cpu_baseline(snap, scaling, cfg, args.cpu_seconds)
+    m = grrt.model_struct(grrt.HybridSynchrotronCoefficients(), cfg.transfer.observing_frequency_hz, scaling)
+    per_mean = statistics.mean(per)
+    line = {
+        "metric": "pixels/s", "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"physical polarized GRRT, default render config: {cfg.width}x{cfg.height} pixels, "
+                               "camera r=55M i=65deg FOV 32deg, RK4 step 0.06, 5000 steps, RK2 Stokes steps, "
+                               f"Hybrid synchrotron at 230 GHz, seeded {G['nr']}x{G['ntheta']}x{G['nphi']} snapshot",
+                   "pixels_per_step": pixels, "emitting_segments_per_step": segments, "rk4_steps_per_step": steps,
+                   "l2": "snapshot (11.5 MB) resident in L2; the work is per-segment arithmetic",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
+        "roofline": exp_roofline(segments, per_mean * 1e-3, peaks, exps_per_evaluation(m), "grrt_kernel"),
+        "cpu_baseline": cpu,
+        "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
+    }
+    if world > 1:
+        import torch.distributed as td
+
+        td.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def grrt_cpu_baseline(snap, scaling, cfg, target_s: float) -> dict:
+    """The float64 oracle (oracle/grrt.py, one core) on pixels of the image's middle row."""
+    sys.path.insert(0, str(REPO))
+    from blackhole_native import grrt
+    from oracle import grrt as OG
+    from oracle import oracle as O
+
+    cam = cfg.camera
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = snap.spin_a, cam.r, cam.theta, cam.phi
+    v.fov_y_deg, v.roll_deg, v.width, v.height = cam.fov_y_degrees, cam.roll_degrees, cfg.width, cfg.height
+    fields = grrt.snapshot_fields(snap)
+    sc = {"rho_cgs_per_code": scaling.rho_cgs_per_code, "b_gauss_per_code": scaling.b_gauss_per_code}
+    t0 = time.perf_counter()
+    n = segs = 0
+    py = cfg.height // 2
+    while n < cfg.width and (n == 0 or time.perf_counter() - t0 < target_s):
+        px = (cfg.width // 2 + n) % cfg.width
+        _, (_, emit, _) = OG.trace_pixel(v, fields, snap.r, snap.theta, snap.phi, sc,
+                                         cfg.transfer.observing_frequency_hz, cfg.step, cfg.max_steps,
+                                         cfg.escape_radius, length_cm=scaling.rg_cm, px=px, py=py)
+        n += 1
+        segs += emit
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "pixels/s", "cores": 1, "kind": "port",
+            "sample": f"float64 oracle (oracle/grrt.py, one core): {n} pixels of the middle row "
+                      f"({segs} emitting segments) in {dt:.2f} s"}
+
+
+def _scaled_traffic(summary: Path, scale: float) -> float | None:
+    t = profiled_traffic(summary)
+    return None if t is None else t * scale
+
+
+def _uuid(device):
+    import torch
+
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+    except Exception:
+        return None
+
+
+def _lib_check(rc):
+    from blackhole_native import _lib
+
+    _lib.check(rc)
+
+
 def bench_reference(args) -> dict | None:
     rank, world, _ = dist_env()
     if rank != 0:
@@ -514,17 +841,23 @@ def main(argv=None) -> int:
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")
     ap.add_argument("--tune", action="store_true", help="run the launch-shape autotuner on the workload and exit")
-    ap.add_argument("--workload", choices=["image", "views"], default="image",
-                    help="image: the 1024x1024 single view (default); views: many uneven views in one launch")
+    ap.add_argument("--workload", choices=["image", "views", "precompute", "grrt"], default="image",
+                    help="image: the 1024x1024 single view (default); views: many uneven views in one launch; "
+                         "precompute: coefficient bricks from a snapshot; grrt: the physical polarized renderer")
     ap.add_argument("--n-views", type=int, default=256)
     ap.add_argument("--side", type=int, default=0,
-                    help="render side x side rays of the same scene instead of 1024x1024 (profiling only)")
+                    help="profiling only: image workload side x side rays; precompute nr = side; grrt image "
+                         "side x side*9/16")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, whatever is asked
     if args.impl == "reference":
         line = bench_reference(args)
     elif args.workload == "views":
         line = bench_views(args)
+    elif args.workload == "precompute":
+        line = bench_precompute(args)
+    elif args.workload == "grrt":
+        line = bench_grrt(args)
     else:
         line = bench_ours(args)
     if line is not None:

@@ -18,7 +18,7 @@ RAY_STATUS = ("max_steps", "captured", "escaped", "invalid", "optically_thick")
 
 # Every symbol include/blackhole_native.h declares.
 EXPORTED = (
-    "bhn_core_version", "bhn_last_error", "bhn_device_info", "bhn_fp32_peak_probe",
+    "bhn_core_version", "bhn_last_error", "bhn_device_info", "bhn_fp32_peak_probe", "bhn_fp64_peak_probe",
     "bhn_stokes_rk2_brick", "bhn_stokes_exact_brick", "bhn_sample_brick_trilinear", "bhn_sample_and_step_stokes",
     "bhn_sample_brick_valid_mask", "bhn_check_values",
     "bhn_brick_tables_bytes", "bhn_brick_build_tables", "bhn_brick_pack", "bhn_brick_locate",
@@ -110,6 +110,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "bhn_last_error": ([], ctypes.c_char_p),
         "bhn_device_info": ([vp, vp, vp, vp], ctypes.c_int),
         "bhn_fp32_peak_probe": ([vp, i32, i32, vp, vp], ctypes.c_int),
+        "bhn_fp64_peak_probe": ([vp, i32, i32, i32, vp, vp], ctypes.c_int),
         "bhn_stokes_rk2_brick": ([vp, i64, d, vp, i64, vp, vp], ctypes.c_int),
         "bhn_stokes_exact_brick": ([vp, i64, d, vp, i64, vp, vp], ctypes.c_int),
         "bhn_sample_brick_trilinear": ([vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp], ctypes.c_int),

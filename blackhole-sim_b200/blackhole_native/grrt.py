@@ -11,7 +11,7 @@ kernel (``bhn_grrt_render``, one warp per ray).
 The configuration, camera, snapshot and scaling arguments are duck-typed: the
 reference's own ``PolarizedRenderConfig`` / ``LocalCamera`` /
 ``GRMHDSnapshot`` / ``PhysicalScaling`` objects work, and so do this module's
-mirrors of the first two.
+mirrors of them (``seeded_snapshot`` makes a synthetic snapshot).
 """
 
 from __future__ import annotations
@@ -76,6 +76,64 @@ class PolarizedRenderConfig:
     tone_map: bool = True
 
 
+@dataclass
+class Snapshot:
+    """The fields of ``grmhd.GRMHDSnapshot`` (grmhd.py:54-68) the GPU paths read:
+    grids, rho, Theta_e, pressure [nr, nt, np] and b^mu, u^mu [nr, nt, np, 4]."""
+
+    r: np.ndarray
+    theta: np.ndarray
+    phi: np.ndarray
+    rho: np.ndarray
+    theta_e: np.ndarray
+    pressure: np.ndarray
+    b_con: np.ndarray
+    u_con: np.ndarray
+    spin_a: float
+
+
+@dataclass(frozen=True)
+class PhysicalScaling:
+    """calibration.py:48-54 (the unit conversions; rg_cm as calibration.py:107-109)."""
+
+    mass_bh_g: float
+    distance_cm: float
+    rho_cgs_per_code: float
+    b_gauss_per_code: float
+    ion_to_electron_temperature_ratio: float = 3.0
+    mean_molecular_weight_per_electron: float = 1.0
+    flux_scale_jy: float = 1.0
+
+    @property
+    def rg_cm(self) -> float:
+        return G_CGS * self.mass_bh_g / (C_CGS * C_CGS)
+
+
+def seeded_snapshot(nr: int = 64, nt: int = 32, nphi: int = 64, spin_a: float = 0.9375, seed: int = 0) -> Snapshot:
+    """A seeded GRMHD-like snapshot: r geometric from 1.05 r_+ to 40 M, theta
+    cell-centred on (0, pi), phi uniform on [0, 2 pi); torus density
+    exp(-(r - 8)^2 / 8 - 4 cos^2 theta) with log-normal noise (sigma 0.2),
+    Theta_e log-uniform on [1, 60], pressure rho Theta_e, Gaussian b^mu and a
+    slowly rotating flow u = (1, 0, 0, 0.5 r^-1.5)."""
+    if min(nr, nt, nphi) < 2:
+        raise ValueError("snapshot grids need at least 2 points per axis")
+    rng = np.random.default_rng(seed)
+    r_plus = 1.0 + math.sqrt(max(1.0 - spin_a * spin_a, 0.0))
+    r = np.geomspace(1.05 * r_plus, 40.0, nr)
+    theta = (np.arange(nt) + 0.5) * math.pi / nt
+    phi = np.linspace(0.0, 2.0 * math.pi, nphi, endpoint=False)
+    shape = (nr, nt, nphi)
+    rho = np.exp(-((r[:, None, None] - 8.0) ** 2) / 8.0 - 4.0 * np.cos(theta)[None, :, None] ** 2) \
+        * np.exp(rng.normal(0.0, 0.2, shape))
+    theta_e = np.exp(rng.uniform(0.0, math.log(60.0), shape))
+    b_con = rng.normal(0.0, 1.0, shape + (4,))
+    u_con = np.zeros(shape + (4,))
+    u_con[..., 0] = 1.0
+    u_con[..., 3] = 0.5 * r[:, None, None] ** -1.5
+    return Snapshot(r=r, theta=theta, phi=phi, rho=rho, theta_e=theta_e, pressure=rho * theta_e, b_con=b_con,
+                    u_con=u_con, spin_a=float(spin_a))
+
+
 class GrrtConfigStruct(ctypes.Structure):
     """``bhn_grrt_config``."""
 
@@ -127,22 +185,39 @@ def _length_cm(transfer, scaling) -> float:
     return float(rg)
 
 
+class DeviceSnapshot:
+    """A snapshot's grids and [nr][nt][np][11] field records resident on the
+    device, for rendering many images of one snapshot without re-uploading."""
+
+    def __init__(self, snapshot, device: torch.device | None = None):
+        device = device or dev.require_cuda()
+        for name in ("r", "theta", "phi"):
+            g = np.asarray(getattr(snapshot, name), dtype=np.float64)
+            if g.ndim != 1 or g.size < 2 or np.any(np.diff(g) <= 0.0):
+                raise ValueError(f"{name} grid must be a strictly increasing 1-D array")
+        self.device = device
+        self.spin_a = float(snapshot.spin_a)
+        self.grids = [torch.as_tensor(np.ascontiguousarray(np.asarray(getattr(snapshot, n), dtype=np.float64)),
+                                      device=device) for n in ("r", "theta", "phi")]
+        self.fields = torch.as_tensor(snapshot_fields(snapshot), device=device)
+
+    @property
+    def upload_bytes(self) -> int:
+        return int(self.fields.numel() * 8 + sum(g.numel() for g in self.grids) * 8)
+
+
 def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diagnostics: bool = False,
-                               device: torch.device | None = None):
+                               device: torch.device | None = None, out: torch.Tensor | None = None):
     """(H, W, 4) float64 Stokes image on the device (and (H, W, 8) diagnostics,
-    columns ``DIAGNOSTICS``, when asked)."""
+    columns ``DIAGNOSTICS``, when asked).  ``snapshot`` is a host snapshot or a
+    ``DeviceSnapshot``; ``out`` an optional preallocated (H, W, 4) float64
+    device tensor."""
     L = _declare()
-    device = device or dev.require_cuda()
-    for name in ("r", "theta", "phi"):
-        g = np.asarray(getattr(snapshot, name), dtype=np.float64)
-        if g.ndim != 1 or g.size < 2 or np.any(np.diff(g) <= 0.0):
-            raise ValueError(f"{name} grid must be a strictly increasing 1-D array")
-    grids = [torch.as_tensor(np.ascontiguousarray(np.asarray(getattr(snapshot, n), dtype=np.float64)), device=device)
-             for n in ("r", "theta", "phi")]
-    fields = torch.as_tensor(snapshot_fields(snapshot), device=device)
+    ds = snapshot if isinstance(snapshot, DeviceSnapshot) else DeviceSnapshot(snapshot, device)
+    device = ds.device
     cam = cfg.camera
     v = _lib.ViewStruct()
-    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = float(snapshot.spin_a), float(cam.r), float(cam.theta), float(cam.phi)
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = ds.spin_a, float(cam.r), float(cam.theta), float(cam.phi)
     v.fov_y_deg, v.roll_deg = float(cam.fov_y_degrees), float(getattr(cam, "roll_degrees", 0.0))
     v.h_scale, v.h_min, v.h_max = 0.02, 1e-3, 1.0  # unused by the fixed-step loop
     v.escape_radius, v.affine_to_length_cm, v.max_optical_depth = float(cfg.escape_radius), 1.0, 30.0
@@ -160,11 +235,16 @@ def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diag
     nbytes = int(L.bhn_render_scratch_bytes(1))
     scratch = torch.zeros(nbytes // 8 + 64, dtype=torch.float64, device=device)
     sp = (dev.ptr(scratch) + 255) & ~255
-    out = torch.empty((v.height, v.width, 4), dtype=torch.float64, device=device)
+    if out is None:
+        out = torch.empty((v.height, v.width, 4), dtype=torch.float64, device=device)
+    elif (tuple(out.shape) != (v.height, v.width, 4) or out.dtype != torch.float64 or out.device != device
+          or not out.is_contiguous()):
+        raise ValueError("out must be a contiguous (H, W, 4) float64 tensor on the snapshot's device")
     diag = torch.empty((v.height, v.width, 8), dtype=torch.float64, device=device) if diagnostics else None
-    _lib.check(L.bhn_grrt_render(dev.ptr(fields), dev.ptr(grids[0]), grids[0].numel(), dev.ptr(grids[1]),
-                                 grids[1].numel(), dev.ptr(grids[2]), grids[2].numel(), ctypes.byref(v), ctypes.byref(m),
-                                 ctypes.byref(c), sp, nbytes, dev.ptr(out), dev.ptr(diag), dev.stream_ptr()))
+    g = ds.grids
+    _lib.check(L.bhn_grrt_render(dev.ptr(ds.fields), dev.ptr(g[0]), g[0].numel(), dev.ptr(g[1]), g[1].numel(),
+                                 dev.ptr(g[2]), g[2].numel(), ctypes.byref(v), ctypes.byref(m), ctypes.byref(c), sp,
+                                 nbytes, dev.ptr(out), dev.ptr(diag), dev.stream_ptr()))
     return (out, diag) if diagnostics else out
 
 

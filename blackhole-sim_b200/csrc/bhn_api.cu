@@ -263,6 +263,33 @@ __global__ void __launch_bounds__(256) fp32_peak_kernel(float *out, int iters, f
     if (s == 12345.678f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
 }
 
+// FP64 probes: FMA chains as above, or 8 chains of x <- exp(-x) (values stay
+// in (0, 1], converging to the omega constant; no overflow, no denormals).
+__global__ void __launch_bounds__(256) fp64_peak_kernel(double *out, int iters, int mode, double seed) {
+    double a0 = seed + threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+    double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+    if (mode == 0) {
+        const double m = 0.999999, c = 1e-9;
+        for (int i = 0; i < iters; ++i) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+                a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+                a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+            }
+        }
+    } else {
+        for (int i = 0; i < iters; ++i) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                a0 = exp(-a0); a1 = exp(-a1); a2 = exp(-a2); a3 = exp(-a3);
+                a4 = exp(-a4); a5 = exp(-a5); a6 = exp(-a6); a7 = exp(-a7);
+            }
+        }
+    }
+    const double s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (s == 12345.678) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
+}
+
 static inline unsigned grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     int64_t cap = (int64_t)(sm_count_current_device() > 0 ? sm_count_current_device() : 148) * 16;
@@ -384,6 +411,19 @@ int bhn_fp32_peak_probe(float *scratch, int32_t iters, int32_t blocks_per_sm, in
     fp32_peak_kernel<<<blocks, threads, 0, as_stream(stream)>>>(scratch, iters, 0.5f);
     BHN_LAUNCH_CHECK("fp32_peak_kernel");
     if (flops) *flops = (int64_t)blocks * threads * iters * 16 * 8 * 2;
+    return BHN_OK;
+}
+
+int bhn_fp64_peak_probe(double *scratch, int32_t iters, int32_t blocks_per_sm, int32_t mode, int64_t *ops,
+                        void *stream) {
+    const int sms = sm_count_current_device();
+    if (sms <= 0) return fail(BHN_ERR_CUDA, "cannot query the SM count");
+    if (iters < 1 || blocks_per_sm < 1 || blocks_per_sm > 32) return fail(BHN_ERR_VALUE, "bad probe size");
+    if (mode != 0 && mode != 1) return fail(BHN_ERR_VALUE, "probe mode must be 0 (fma) or 1 (exp)");
+    const int threads = 256, blocks = sms * blocks_per_sm;
+    fp64_peak_kernel<<<blocks, threads, 0, as_stream(stream)>>>(scratch, iters, mode, 0.5);
+    BHN_LAUNCH_CHECK("fp64_peak_kernel");
+    if (ops) *ops = (int64_t)blocks * threads * iters * (mode == 0 ? 16 * 8 * 2 : 4 * 8);
     return BHN_OK;
 }
 

@@ -33,6 +33,7 @@ struct GrrtParams {
     int max_steps, exact_step;
     double *out;                // [rays][4] Stokes
     double *diag;               // optional [rays][8]: tau, emit, valid, faraday depth, g min, g max, steps, status
+    unsigned long long *queue;  // next ray to hand out (zeroed before the launch)
 };
 
 __device__ __forceinline__ void rk4_state(const double y[5], double h, double a, double pt, double pphi, double yn[5]) {
@@ -51,34 +52,62 @@ __device__ __forceinline__ void rk4_state(const double y[5], double h, double a,
     yn[4] = y[4] + h6 * (((k1.pth + 2.0 * k2.pth) + 2.0 * k3.pth) + k4.pth);
 }
 
+// The state a ray carries across its segments, one copy per warp in shared
+// memory: the lanes hold identical values (they run the same arithmetic, and
+// the butterfly sums of the coefficient integrals give every lane the same
+// bits), so every lane stores and reloads the same numbers.  Keeping it out of
+// registers while the warp evaluates a segment's synchrotron integrals leaves
+// those registers to the integrals.
+struct RayState {
+    double y[5], S[4], tau, fd, gmin, gmax, prev_r, pt, pphi;
+};
+
 __global__ void __launch_bounds__(128, 4) grrt_kernel(const __grid_constant__ GrrtParams P) {
     __shared__ synch::TableSmem T;
+    __shared__ RayState ray_state[4];
     synch::load_table(T, P.M);
     __syncthreads();
     const ViewDev &v = *P.view;
     const int lane = threadIdx.x & 31;
+    volatile RayState &st = ray_state[threadIdx.x >> 5];
     const int64_t rays = (int64_t)v.crop_w * v.crop_h;
-    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t ray = warp0; ray < rays; ray += warps) {
+    // Rays differ by orders of magnitude in emitting segments: a persistent
+    // grid whose warps take the next ray from one counter keeps every warp busy
+    // until the last rays.
+    for (;;) {
+        unsigned long long next = 0;
+        if (lane == 0) next = atomicAdd(P.queue, 1ull);
+        const int64_t ray = (int64_t)__shfl_sync(0xffffffffu, next, 0);
+        if (ray >= rays) break;
         const int px = v.x0 + (int)(ray % v.crop_w), py = v.y0 + (int)(ray / v.crop_w);
-        const CameraRay cam = camera_ray(v, px, py);
-        double y[5] = {v.r_obs, v.theta_obs, v.phi_obs, cam.pr, cam.pth};
-        const double pt = cam.pt, pphi = cam.pphi, a = v.a;
-        double S[4] = {0.0, 0.0, 0.0, 0.0};
-        double tau = 0.0, fd = 0.0, gmin = INFINITY, gmax = 0.0;
-        int emit = 0, valid = 0, steps = 0, status = BHN_RAY_MAX_STEPS;
-        double prev_r = y[0];
-        bool done = !v.valid;
-        if (!v.valid) status = BHN_RAY_INVALID;
-        for (int i = 1; i <= P.max_steps && !done; ++i) {
-            double yn[5];
+        {
+            const CameraRay cam = camera_ray(v, px, py);
+            st.y[0] = v.r_obs;
+            st.y[1] = v.theta_obs;
+            st.y[2] = v.phi_obs;
+            st.y[3] = cam.pr;
+            st.y[4] = cam.pth;
+            st.pt = cam.pt;
+            st.pphi = cam.pphi;
+            for (int k = 0; k < 4; ++k) st.S[k] = 0.0;
+            st.tau = 0.0;
+            st.fd = 0.0;
+            st.gmin = INFINITY;
+            st.gmax = 0.0;
+            st.prev_r = v.r_obs;
+        }
+        int emit = 0, valid = 0, steps = 0, status = v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID;
+        for (int i = 1; i <= P.max_steps && v.valid; ++i) {
+            const double a = v.a, pt = st.pt, pphi = st.pphi;
+            double y[5], yn[5];
+            for (int k = 0; k < 5; ++k) y[k] = st.y[k];
             rk4_state(y, P.step, a, pt, pphi, yn);
             steps = i;
             if (!(isfinite(yn[0]) && isfinite(yn[1]) && isfinite(yn[2]) && isfinite(yn[3]) && isfinite(yn[4]))) {
                 status = BHN_RAY_INVALID;  // kerr.py:364-366: not stored, no segment
                 break;
             }
+            for (int k = 0; k < 5; ++k) st.y[k] = yn[k];
             // segment (y, yn): polarized_transfer.py:103-143
             const double mr = 0.5 * (y[0] + yn[0]), mth = 0.5 * (y[1] + yn[1]), mph = 0.5 * (y[2] + yn[2]);
             const double mpr = 0.5 * (y[3] + yn[3]), mpth = 0.5 * (y[4] + yn[4]);
@@ -105,59 +134,63 @@ __global__ void __launch_bounds__(128, 4) grrt_kernel(const __grid_constant__ Gr
                     }
                     const double chi = b_code > 0.0 ? atan2(b3, b2) : 0.0;
                     const double te = fmax(f[1], 1.0e-8), b = fmax(b_code * P.M.b_unit, 0.0);
+                    const double jf = g * g * P.flux_scale, kf = 1.0 / fmax(g, 1.0e-300);
+                    const double dr = yn[0] - y[0], dth = yn[1] - y[1], dph = yn[2] - y[2];
+                    const double dl = sqrt((dr * dr + dth * dth) + dph * dph);
+                    const double ds = P.length_cm * fmax(e_emit, 0.0) * fmax(dl, 1.0e-14);
+                    st.gmin = fmin(st.gmin, g);
+                    st.gmax = fmax(st.gmax, g);
                     double c[11];
                     synch::coefficients(T, P.M, n_e, te, b, cos_los, chi, P.nu / g, c);
-                    const double jf = g * g * P.flux_scale, kf = 1.0 / fmax(g, 1.0e-300);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) c[k] *= jf;
 #pragma unroll
                     for (int k = 4; k < 11; ++k) c[k] *= kf;
-                    const double dr = yn[0] - y[0], dth = yn[1] - y[1], dph = yn[2] - y[2];
-                    const double dl = sqrt((dr * dr + dth * dth) + dph * dph);
-                    const double ds = P.length_cm * fmax(e_emit, 0.0) * fmax(dl, 1.0e-14);
+                    double S[4];
+                    for (int k = 0; k < 4; ++k) S[k] = st.S[k];
                     if (P.exact_step)
                         stokes_step_exact(S, c, ds);
                     else
                         stokes_step_rk2_exact(S, c, ds);
-                    tau += fmax(c[4], 0.0) * ds;
-                    fd += (fabs(c[8]) + fabs(c[9]) + fabs(c[10])) * ds;
+                    for (int k = 0; k < 4; ++k) st.S[k] = S[k];
+                    const double tau = st.tau + fmax(c[4], 0.0) * ds;
+                    st.tau = tau;
+                    st.fd = st.fd + (fabs(c[8]) + fabs(c[9]) + fabs(c[10])) * ds;
                     ++emit;
-                    gmin = fmin(gmin, g);
-                    gmax = fmax(gmax, g);
-                    if (tau >= P.max_tau) done = true;
+                    if (tau >= P.max_tau) {
+                        status = BHN_RAY_OPAQUE;
+                        break;
+                    }
                 }
             }
-            for (int k = 0; k < 5; ++k) y[k] = yn[k];
-            if (done) {
-                status = BHN_RAY_OPAQUE;
-                break;
-            }
             // kerr.py:370-378
-            if (y[0] <= v.r_capture) {
+            const double r = st.y[0];
+            if (r <= v.r_capture) {
                 status = BHN_RAY_CAPTURED;
                 break;
             }
-            if (y[0] > P.escape_radius && y[0] > prev_r) {
+            if (r > P.escape_radius && r > st.prev_r) {
                 status = BHN_RAY_ESCAPED;
                 break;
             }
-            prev_r = y[0];
+            st.prev_r = r;
         }
         if (lane == 0) {
             const int64_t o = v.out_offset + (int64_t)(py - v.y0) * v.crop_w + (px - v.x0);
-            for (int k = 0; k < 4; ++k) P.out[4 * o + k] = S[k];
+            for (int k = 0; k < 4; ++k) P.out[4 * o + k] = st.S[k];
             if (P.diag) {
                 double *d = P.diag + 8 * o;
-                d[0] = tau;
+                d[0] = st.tau;
                 d[1] = emit;
                 d[2] = valid;
-                d[3] = fd;
-                d[4] = gmin < INFINITY ? gmin : 0.0;
-                d[5] = gmax;
+                d[3] = st.fd;
+                d[4] = st.gmin < INFINITY ? st.gmin : 0.0;
+                d[5] = st.gmax;
                 d[6] = steps;
                 d[7] = status;
             }
         }
+        __syncwarp();  // every lane is done with this ray's state before the next ray overwrites it
     }
 }
 
@@ -206,10 +239,13 @@ extern "C" int bhn_grrt_render(const double *fields, const double *r_grid, int32
     P.diag = diag;
     const int64_t rays = (int64_t)view->crop_w * view->crop_h;
     if (rays <= 0) return BHN_OK;
-    int dev = 0, sms = 148;
+    int dev = 0, sms = 148, per_sm = 0;
     BHN_CUDA_TRY(cudaGetDevice(&dev));
     BHN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int64_t blocks = std::min<int64_t>((rays + 3) / 4, (int64_t)sms * 16);
+    BHN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grrt_kernel, 128, 0));
+    const int64_t blocks = std::min<int64_t>((rays + 3) / 4, (int64_t)sms * std::max(per_sm, 1));
+    P.queue = reinterpret_cast<unsigned long long *>(sc + L.queue);
+    BHN_CUDA_TRY(cudaMemsetAsync(P.queue, 0, sizeof(unsigned long long), as_stream(stream)));
     grrt_kernel<<<(unsigned)blocks, 128, 0, as_stream(stream)>>>(P);
     BHN_LAUNCH_CHECK("grrt_kernel");
     return BHN_OK;

@@ -30,7 +30,7 @@ struct PrecomputeParams {
     int out_bytes;
 };
 
-__global__ void __launch_bounds__(128) precompute_kernel(const __grid_constant__ PrecomputeParams P) {
+__global__ void __launch_bounds__(128, 6) precompute_kernel(const __grid_constant__ PrecomputeParams P) {
     __shared__ TableSmem T;
     load_table(T, P.M);
     __syncthreads();

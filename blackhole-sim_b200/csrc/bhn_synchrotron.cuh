@@ -63,6 +63,7 @@ struct Model {
 
 struct TableSmem {
     double lx[kTable], lF[kTable], lG[kTable], sF[kTable], sG[kTable];
+    double inv;  // (kTable - 1) / (lx[last] - lx[0]): knots per unit of log x
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -72,22 +73,23 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // numpy.interp on the log-log table (synchrotron.py:165-172): knot j with
-// lx[j] <= x < lx[j + 1]; x at or past the last knot takes the last value.
+// lx[j] <= x < lx[j + 1]; x at or past the last knot takes the last value,
+// x below the first the first (d = 0 there).  Every lane takes exactly two
+// exp calls whatever its x, so a warp never runs the two cases one after the
+// other.
 __device__ __forceinline__ void kernel_lookup(const TableSmem &T, double lx, double &F, double &G) {
-    lx = fmin(fmax(lx, T.lx[0]), T.lx[kTable - 1]);
-    if (lx >= T.lx[kTable - 1]) {
-        F = exp(T.lF[kTable - 1]);
-        G = exp(T.lG[kTable - 1]);
-        return;
-    }
-    const double inv = (double)(kTable - 1) / (T.lx[kTable - 1] - T.lx[0]);
-    int j = (int)((lx - T.lx[0]) * inv);
+    const double lo = T.lx[0], hi = T.lx[kTable - 1];
+    const bool past = lx >= hi;
+    lx = fmin(fmax(lx, lo), hi);
+    int j = (int)((lx - lo) * T.inv);
     j = max(0, min(j, kTable - 2));
     while (j > 0 && lx < T.lx[j]) --j;
     while (j < kTable - 2 && lx >= T.lx[j + 1]) ++j;
     const double d = __dsub_rn(lx, T.lx[j]);
-    F = exp(__dadd_rn(__dmul_rn(T.sF[j], d), T.lF[j]));
-    G = exp(__dadd_rn(__dmul_rn(T.sG[j], d), T.lG[j]));
+    const double aF = past ? T.lF[kTable - 1] : __dadd_rn(__dmul_rn(T.sF[j], d), T.lF[j]);
+    const double aG = past ? T.lG[kTable - 1] : __dadd_rn(__dmul_rn(T.sG[j], d), T.lG[j]);
+    F = exp(aF);
+    G = exp(aG);
 }
 
 // numpy.geomspace(start, stop, n)[i] (logspace of a linspace; exact end points).
@@ -118,10 +120,23 @@ __device__ inline Integrals integrate(const TableSmem &T, const Component &C, bo
     const double ls = log10(g0), step = (log10(g1) - ls) / (double)(n - 1);
     const double inv_te = 1.0 / fmax(theta_e, 1.0e-12);
     Integrals acc = {0.0, 0.0, 0.0};
-    for (int i = lane; i < n; i += 32) {
-        const double xi = geom_node(g0, g1, ls, step, i, n);
-        const double xm = i > 0 ? geom_node(g0, g1, ls, step, i - 1, n) : xi;
-        const double xp = i < n - 1 ? geom_node(g0, g1, ls, step, i + 1, n) : xi;
+    // Each lane evaluates one node per chunk of 32 (the next chunk's one step
+    // ahead); the trapezoid's neighbours come from the adjacent lanes.
+    double x_cur = geom_node(g0, g1, ls, step, lane, n), x_last = 0.0;
+    for (int base0 = 0; base0 < n; base0 += 32) {
+        const int i = base0 + lane;
+        const double x_next = geom_node(g0, g1, ls, step, i + 32, n);
+        double xm = __shfl_up_sync(0xffffffffu, x_cur, 1);
+        double xp = __shfl_down_sync(0xffffffffu, x_cur, 1);
+        const double next0 = __shfl_sync(0xffffffffu, x_next, 0);
+        if (lane == 0) xm = x_last;   // node base0 - 1 (previous chunk's lane 31)
+        if (lane == 31) xp = next0;   // node base0 + 32
+        x_last = __shfl_sync(0xffffffffu, x_cur, 31);
+        const double xi = x_cur;
+        x_cur = x_next;
+        if (i >= n) continue;
+        if (i == 0) xm = xi;
+        if (i == n - 1) xp = xi;
         double gamma, c;
         if (thermal) {
             gamma = 1.0 + xi;
@@ -195,6 +210,7 @@ __device__ __forceinline__ void load_table(TableSmem &T, const Model &M) {
         T.sF[i] = M.sF[i];
         T.sG[i] = M.sG[i];
     }
+    if (threadIdx.x == 0) T.inv = (double)(kTable - 1) / (M.lx[kTable - 1] - M.lx[0]);
 }
 
 // The 11 coefficients of the model (synchrotron.py:248-325) for one local

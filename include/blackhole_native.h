@@ -63,6 +63,14 @@ int bhn_device_info(int32_t *sm_count, int32_t *cc_major, int32_t *cc_minor, int
  * written in practice). */
 int bhn_fp32_peak_probe(float *scratch, int32_t iters, int32_t blocks_per_sm, int64_t *flops, void *stream);
 
+/* FP64 throughput probe, the denominator of the synchrotron kernels' rooflines
+ * (a measurement aid like the FP32 probe).  mode 0: iters * 128 FP64 FMAs per
+ * thread, *ops = FLOP (2 per FMA); mode 1: iters * 32 double-precision exp()
+ * calls per thread in 8 independent chains, *ops = exp evaluations.  Same
+ * launch shape and scratch size (doubles) as bhn_fp32_peak_probe. */
+int bhn_fp64_peak_probe(double *scratch, int32_t iters, int32_t blocks_per_sm, int32_t mode, int64_t *ops,
+                        void *stream);
+
 /* ---- plugin micro-kernels (float64, bit-exact with the reference) -------- */
 
 /* Replaces stokes_rk2_brick (native/core/src/lib.rs:227-279).  coeffs: cells*11,

@@ -135,3 +135,25 @@ def test_device_validation_messages():
     dc2[3] = float("nan")
     with pytest.raises(ValueError, match="coeffs must contain only finite values"):
         bn.stokes_rk2_brick(dc2, 0.1, torch.zeros(4, device="cuda", dtype=torch.float64))
+
+
+def test_throughput_probes_run_and_count():
+    """The FP32 / FP64 throughput probes (roofline denominators) launch, report
+    their operation counts and reject a bad mode."""
+    import ctypes
+
+    from blackhole_native import _lib
+
+    L = _lib.lib()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    scratch = torch.empty(sms * 256 * 2, dtype=torch.float64, device="cuda")
+    ops = ctypes.c_int64()
+    _lib.check(L.bhn_fp32_peak_probe(scratch.data_ptr(), 2, 1, ctypes.byref(ops), None))
+    assert ops.value == sms * 256 * 2 * 16 * 8 * 2
+    _lib.check(L.bhn_fp64_peak_probe(scratch.data_ptr(), 2, 1, 0, ctypes.byref(ops), None))
+    assert ops.value == sms * 256 * 2 * 16 * 8 * 2
+    _lib.check(L.bhn_fp64_peak_probe(scratch.data_ptr(), 3, 1, 1, ctypes.byref(ops), None))
+    assert ops.value == sms * 256 * 3 * 4 * 8
+    torch.cuda.synchronize()
+    assert L.bhn_fp64_peak_probe(scratch.data_ptr(), 2, 1, 2, ctypes.byref(ops), None) != 0
+    assert b"probe mode" in L.bhn_last_error()

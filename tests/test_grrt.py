@@ -100,3 +100,48 @@ def test_gpu_larger_image_against_oracle(golden):
         assert e == diag[py, px, 1] and va == diag[py, px, 2]
         assert _rel(img[py, px], S) <= 1e-10 if np.any(S) else not np.any(img[py, px])
         assert abs(tau - diag[py, px, 0]) <= 1e-10 * max(tau, 1e-300)
+
+
+def test_seeded_snapshot_is_deterministic():
+    from blackhole_native import grrt
+
+    a, b = grrt.seeded_snapshot(6, 4, 5, seed=3), grrt.seeded_snapshot(6, 4, 5, seed=3)
+    assert a.rho.shape == (6, 4, 5) and a.b_con.shape == (6, 4, 5, 4) and a.u_con.shape == (6, 4, 5, 4)
+    assert np.array_equal(a.rho, b.rho) and np.array_equal(a.b_con, b.b_con)
+    assert np.all(a.rho > 0) and np.all((a.theta_e >= 1.0) & (a.theta_e <= 60.0))
+    assert np.all(np.diff(a.r) > 0) and a.theta[0] > 0 and a.theta[-1] < np.pi and a.phi[-1] < 2 * np.pi
+    f = grrt.snapshot_fields(a)
+    assert f.shape == (6, 4, 5, 11) and np.array_equal(f[..., 3:7], a.b_con)
+    with pytest.raises(ValueError):
+        grrt.seeded_snapshot(1, 4, 5)
+
+
+@pytest.mark.gpu
+def test_gpu_seeded_snapshot_device_reuse_against_oracle():
+    """A seeded snapshot kept on the device (DeviceSnapshot) renders the same
+    image into a caller's buffer as the host-snapshot call, and its pixels
+    match the oracle."""
+    import torch
+
+    from blackhole_native import grrt
+
+    snap = grrt.seeded_snapshot(16, 8, 12, seed=4)
+    scaling = grrt.PhysicalScaling(mass_bh_g=8.54e39, distance_cm=2.57e22, rho_cgs_per_code=3.0e-18,
+                                   b_gauss_per_code=25.0)
+    cam = grrt.LocalCamera.from_degrees(r=30.0, inclination_degrees=70.0, fov_y_degrees=30.0)
+    cfg = grrt.PolarizedRenderConfig(width=12, height=8, camera=cam, step=0.1, max_steps=900)
+    host = grrt.render_stokes_image(cfg, snap, scaling)
+    ds = grrt.DeviceSnapshot(snap)
+    out = torch.full((8, 12, 4), float("nan"), dtype=torch.float64, device="cuda")
+    got = grrt.render_stokes_image_device(cfg, ds, scaling, out=out)
+    assert got is out and np.array_equal(out.cpu().numpy(), host)
+    with pytest.raises(ValueError, match="out must be"):
+        grrt.render_stokes_image_device(cfg, ds, scaling, out=out[:4])
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = snap.spin_a, cam.r, cam.theta, cam.phi
+    v.fov_y_deg, v.roll_deg, v.width, v.height = cam.fov_y_degrees, cam.roll_degrees, 12, 8
+    sc = dict(rho_cgs_per_code=scaling.rho_cgs_per_code, b_gauss_per_code=scaling.b_gauss_per_code)
+    for px, py in ((5, 3), (11, 0)):
+        S, _ = G.trace_pixel(v, grrt.snapshot_fields(snap), snap.r, snap.theta, snap.phi, sc, 230e9, 0.1, 900, 220.0,
+                             length_cm=scaling.rg_cm, exact=False, px=px, py=py)
+        assert _rel(host[py, px], S) <= 1e-10 if np.any(S) else not np.any(host[py, px])
