@@ -480,6 +480,7 @@ PRECOMPUTE = dict(nr=256, ntheta=128, nphi=256, spin_a=0.9375, seed=5, nu_hz=230
 PRECOMPUTE_PROFILE = REPO / "profiles" / "precompute_kernel_snapshot_2M_cells.md"
 PRECOMPUTE_PROFILE_CELLS = 64 * 128 * 256   # the captured case; its traffic scales with the cells
 GRRT_SNAPSHOT = dict(nr=64, ntheta=32, nphi=64, spin_a=0.9375, seed=0)
+GRRT_PROFILE = REPO / "profiles" / "grrt_kernel_default_image.md"   # the snapshot is read once per launch
 # calibration.PhysicalScaling of a 4.3e6 solar-mass hole at 8.3 kpc with code units rho 3e-18 g/cm^3, B 25 G
 SCALING = dict(mass_bh_g=8.54e39, distance_cm=2.57e22, rho_cgs_per_code=3.0e-18, b_gauss_per_code=25.0)
 
@@ -737,7 +738,8 @@ def bench_grrt(args) -> dict | None:
                    "l2": "snapshot (11.5 MB) resident in L2; the work is per-segment arithmetic",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
-        "roofline": exp_roofline(segments, per_mean * 1e-3, peaks, exps_per_evaluation(m), "grrt_kernel"),
+        "roofline": dict(exp_roofline(segments, per_mean * 1e-3, peaks, exps_per_evaluation(m), "grrt_kernel"),
+                         traffic=profiled_traffic(GRRT_PROFILE)),
         "cpu_baseline": cpu,
         "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
     }
