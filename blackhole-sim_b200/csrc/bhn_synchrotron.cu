@@ -84,6 +84,7 @@ double bessel_k(double nu, double x) {
 
 struct HostTable {
     double lx[kTable], lF[kTable], lG[kTable], sF[kTable], sG[kTable];
+    double lx_tail;
 };
 
 // synchrotron.py:120-172: x = geomspace(1e-8, 1e3, 256), F(x) = 1.25 x^(1/3)
@@ -110,6 +111,12 @@ const HostTable &host_table() {
             t.sF[i] = (t.lF[j + 1] - t.lF[j]) / (t.lx[j + 1] - t.lx[j]);
             t.sG[i] = (t.lG[j + 1] - t.lG[j]) / (t.lx[j + 1] - t.lx[j]);
         }
+        // first knot from which both log F and log G stay below log(kTailValue):
+        // the linear segments in between stay below it too
+        const double tail = std::log(kTailValue);
+        int j0 = kTable;
+        while (j0 > 0 && t.lF[j0 - 1] < tail && t.lG[j0 - 1] < tail) --j0;
+        t.lx_tail = j0 < kTable ? t.lx[j0] : INFINITY;
     });
     return t;
 }
@@ -151,11 +158,13 @@ void pitch_set(int n, PitchSet &ps) {
     double x[kMaxPitch], w[kMaxPitch];
     gauss_legendre(n, x, w);
     ps.n = 0;
+    ps.log_sin_max = 0.0;
     const double pref = std::sqrt(3.0) * kE * kE * kE / (kMe * kC * kC);  // synchrotron.py:185-186 per Gauss
     for (int m = 0; m < n; ++m) {
         const double sin_a = std::sqrt(std::max(0.0, 1.0 - x[m] * x[m]));
         if (!(sin_a > 0.0)) continue;  // Bp = B sin(alpha) <= 0 contributes nothing
         ps.log_sin[ps.n] = std::log(sin_a);
+        ps.log_sin_max = ps.n == 0 ? ps.log_sin[0] : std::max(ps.log_sin_max, ps.log_sin[ps.n]);
         ps.weight[ps.n] = 0.5 * w[m] * pref * sin_a;
         ++ps.n;
     }
@@ -181,6 +190,7 @@ int fill_model(const bhn_synchrotron_model *m, Model &M) {
     std::memcpy(M.lG, t.lG, sizeof t.lG);
     std::memcpy(M.sF, t.sF, sizeof t.sF);
     std::memcpy(M.sG, t.sG, sizeof t.sG);
+    M.lx_tail = t.lx_tail;
     M.rho_unit = m->rho_cgs_per_code;
     M.b_unit = m->b_gauss_per_code;
     M.mu_e_mp = std::max(m->mean_molecular_weight_per_electron * kMp, 1.0e-300);

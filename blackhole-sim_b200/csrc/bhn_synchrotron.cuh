@@ -37,11 +37,13 @@ constexpr double kH = 6.62607015e-27;
 constexpr double kPiD = 3.14159265358979323846;
 
 constexpr int kTable = 256;      // synchrotron.py:158
+constexpr double kTailValue = 1.0e-250;  // F, G below this are dropped with their node (integrate)
 constexpr int kMaxPitch = 64;
 constexpr int kMaxGamma = 4096;
 
 struct PitchSet {
     int n;
+    double log_sin_max;          // the largest log sin(alpha_m) (the pitch with the smallest x)
     double log_sin[kMaxPitch];   // log sin(alpha_m)
     double weight[kMaxPitch];    // 0.5 w_m sqrt(3) e^3 sin(alpha_m) / (m_e c^2): the pitch weight times pref / B
 };
@@ -57,13 +59,15 @@ struct Component {
 // scaling of calibration.py:113-119 (n_e = rho rho_unit / (mu_e m_p), B = |b| b_unit).
 struct Model {
     double lx[kTable], lF[kTable], lG[kTable], sF[kTable], sG[kTable];  // log x knots, log F, log G, slopes
+    double lx_tail;  // from this log x on, F and G are below kTailValue up to the table end (+inf: nowhere)
     double rho_unit, b_unit, mu_e_mp;
     Component th, nt;
 };
 
 struct TableSmem {
     double lx[kTable], lF[kTable], lG[kTable], sF[kTable], sG[kTable];
-    double inv;  // (kTable - 1) / (lx[last] - lx[0]): knots per unit of log x
+    double inv;      // (kTable - 1) / (lx[last] - lx[0]): knots per unit of log x
+    double lx_tail;  // Model::lx_tail
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -155,8 +159,13 @@ __device__ inline Integrals integrate(const TableSmem &T, const Component &C, bo
         }
         const double w = c * f;
         acc.norm += w;
-        if (w != 0.0) {
-            const double two_lg = 2.0 * log(gamma);
+        const double two_lg = w != 0.0 ? 2.0 * log(gamma) : 0.0;
+        // A node whose smallest x (the pitch with the largest sin) already lies
+        // in the table's far tail adds terms below kTailValue times the pitch
+        // weights (< 1e-270): nothing a cell that emits can resolve.  Skipping
+        // it leaves such cells unchanged to the last bit (one that does not
+        // emit at all gets 0 instead of a sum of those terms).
+        if (w != 0.0 && __dsub_rn(__dsub_rn(base, C.pitch.log_sin_max), two_lg) < T.lx_tail) {
             double sI = 0.0, sQ = 0.0;
             for (int m = 0; m < C.pitch.n; ++m) {
                 double F, G;
@@ -210,7 +219,10 @@ __device__ __forceinline__ void load_table(TableSmem &T, const Model &M) {
         T.sF[i] = M.sF[i];
         T.sG[i] = M.sG[i];
     }
-    if (threadIdx.x == 0) T.inv = (double)(kTable - 1) / (M.lx[kTable - 1] - M.lx[0]);
+    if (threadIdx.x == 0) {
+        T.inv = (double)(kTable - 1) / (M.lx[kTable - 1] - M.lx[0]);
+        T.lx_tail = M.lx_tail;
+    }
 }
 
 // The 11 coefficients of the model (synchrotron.py:248-325) for one local
