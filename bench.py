@@ -726,6 +726,8 @@ def bench_grrt(args) -> dict | None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = grrt_cpu_baseline(snap, scaling, cfg, args.cpu_seconds)
     m = grrt.model_struct(grrt.HybridSynchrotronCoefficients(), cfg.transfer.observing_frequency_hz, scaling)
+    chunk = grrt.default_chunk(pixels)
+    launches_per_image = 1 + 3 * (cfg.max_steps // chunk + 2)  # init, then trace / coefficient / transfer rounds
     per_mean = statistics.mean(per)
     line = {
         "metric": "pixels/s", "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps,
@@ -735,10 +737,13 @@ def bench_grrt(args) -> dict | None:
                                "camera r=55M i=65deg FOV 32deg, RK4 step 0.06, 5000 steps, RK2 Stokes steps, "
                                f"Hybrid synchrotron at 230 GHz, seeded {G['nr']}x{G['ntheta']}x{G['nphi']} snapshot",
                    "pixels_per_step": pixels, "emitting_segments_per_step": segments, "rk4_steps_per_step": steps,
+                   "segments_per_ray_and_round": chunk,
                    "l2": "snapshot (11.5 MB) resident in L2; the work is per-segment arithmetic",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
-        "roofline": dict(exp_roofline(segments, per_mean * 1e-3, peaks, exps_per_evaluation(m), "grrt_kernel"),
+        "e2e": e2e, "gpu_launches": args.steps * launches_per_image, "clocks": clk,
+        "roofline": dict(exp_roofline(segments, per_mean * 1e-3, peaks, exps_per_evaluation(m),
+                                      "grrt_coef_kernel (timed: the whole render, all rounds of the trace, "
+                                      "coefficient and transfer kernels)"),
                          traffic=profiled_traffic(GRRT_PROFILE)),
         "cpu_baseline": cpu,
         "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},

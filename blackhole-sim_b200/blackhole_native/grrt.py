@@ -5,8 +5,9 @@ polarized_renderer.py:31-70): per pixel the camera ray, a fixed-step RK4 Kerr
 geodesic (kerr.py:337-384) and ``integrate_polarized_kerr_grrt``
 (polarized_transfer.py:83-145) -- snapshot sampled at every segment's
 midpoint, invariant redshift, synchrotron coefficients of the plasma frame at
-the emitted frequency, exact or RK2 Stokes steps -- all in one FP64 CUDA
-kernel (``bhn_grrt_render``, one warp per ray).
+the emitted frequency, exact or RK2 Stokes steps -- in FP64 CUDA
+(``bhn_grrt_render``: rounds of a thread-per-ray trace kernel, a
+warp-per-segment coefficient kernel and a thread-per-ray transfer kernel).
 
 The configuration, camera, snapshot and scaling arguments are duck-typed: the
 reference's own ``PolarizedRenderConfig`` / ``LocalCamera`` /
@@ -156,6 +157,8 @@ DIAGNOSTICS = ("optical_depth", "emitting_steps", "valid_steps", "faraday_depth_
 
 def _declare() -> ctypes.CDLL:
     L = _lib.lib()
+    L.bhn_grrt_scratch_bytes.argtypes = [ctypes.c_int64, ctypes.c_int32]
+    L.bhn_grrt_scratch_bytes.restype = ctypes.c_int64
     fn = L.bhn_grrt_render
     vp, i32 = ctypes.c_void_p, ctypes.c_int32
     fn.argtypes = [vp, vp, i32, vp, i32, vp, i32, ctypes.POINTER(_lib.ViewStruct), ctypes.POINTER(ModelStruct),
@@ -206,12 +209,22 @@ class DeviceSnapshot:
         return int(self.fields.numel() * 8 + sum(g.numel() for g in self.grids) * 8)
 
 
+SEGMENT_BYTES = 188          # per ray and chunk slot: plasma frame, transfer side data, list index, coefficients
+SCRATCH_BUDGET = 512 << 20   # default scratch: chunk = budget / (rays * SEGMENT_BYTES) within [16, 256]
+
+
+def default_chunk(rays: int) -> int:
+    return int(min(256, max(16, SCRATCH_BUDGET // max(1, rays * SEGMENT_BYTES))))
+
+
 def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diagnostics: bool = False,
-                               device: torch.device | None = None, out: torch.Tensor | None = None):
+                               device: torch.device | None = None, out: torch.Tensor | None = None,
+                               chunk: int | None = None):
     """(H, W, 4) float64 Stokes image on the device (and (H, W, 8) diagnostics,
     columns ``DIAGNOSTICS``, when asked).  ``snapshot`` is a host snapshot or a
     ``DeviceSnapshot``; ``out`` an optional preallocated (H, W, 4) float64
-    device tensor."""
+    device tensor; ``chunk`` the emitting segments listed per ray and round
+    (memory against rounds; the image does not depend on it)."""
     L = _declare()
     ds = snapshot if isinstance(snapshot, DeviceSnapshot) else DeviceSnapshot(snapshot, device)
     device = ds.device
@@ -232,8 +245,12 @@ def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diag
     c.flux_scale = float(getattr(scaling, "flux_scale_jy", 1.0))
     c.max_steps, c.exact_step = int(cfg.max_steps), int(bool(t.use_exact_matrix_step))
     m = model_struct(coeff_model or HybridSynchrotronCoefficients(), t.observing_frequency_hz, scaling)
-    nbytes = int(L.bhn_render_scratch_bytes(1))
-    scratch = torch.zeros(nbytes // 8 + 64, dtype=torch.float64, device=device)
+    rays = v.width * v.height
+    chunk = default_chunk(rays) if chunk is None else int(chunk)
+    if chunk < 1:
+        raise ValueError("chunk must be positive")
+    nbytes = int(L.bhn_grrt_scratch_bytes(rays, chunk))
+    scratch = torch.empty(nbytes // 8 + 64, dtype=torch.float64, device=device)
     sp = (dev.ptr(scratch) + 255) & ~255
     if out is None:
         out = torch.empty((v.height, v.width, 4), dtype=torch.float64, device=device)

@@ -12,10 +12,19 @@
 // rotation), ds = L (-p.u) |d(r, theta, phi)|, and one exact or RK2 Stokes
 // step, until tau reaches the cutoff.
 //
-// One warp owns a ray: all 32 lanes step the geodesic identically (it is cheap
-// next to the coefficients), and the warp evaluates each segment's
-// synchrotron integrals together (bhn_synchrotron.cuh).  Segments are
-// integrated as the ray is traced; the trace's own stopping rules end it.
+// Wavefront form.  The geodesic is a long chain of dependent FP64 steps per
+// ray and the coefficients are ~10^4 independent exp() evaluations per
+// emitting segment, so they run as separate kernels, in rounds:
+//   trace_kernel     one thread per ray: continues its RK4 geodesic until it
+//                    has produced `chunk` emitting segments (or the trace
+//                    ends), appending each segment's plasma frame to a list;
+//   coef_kernel      one warp per listed segment: the synchrotron integrals
+//                    (bhn_synchrotron.cuh) at full occupancy;
+//   transfer_kernel  one thread per ray: its segments' Stokes steps in order,
+//                    the optical-depth cutoff, the result when the ray ends.
+// A ray whose optical depth crosses the cutoff ends at that segment (its
+// trace may have run up to chunk - 1 segments further; those are discarded),
+// so every result equals the segment-by-segment loop's.
 
 #include "bhn_exact.cuh"
 #include "bhn_synchrotron.cuh"
@@ -23,17 +32,53 @@
 
 namespace bhn {
 
-struct GrrtParams {
-    synch::Model M;
+struct GrrtRay {
+    double y[5], pt, pphi, prev_r;     // BL r, theta, phi, p_r, p_theta; conserved p_t, p_phi; r of the last step
+    double S[4], tau, fd, gmin, gmax;  // Stokes vector, optical and Faraday depth, redshift range
+    int32_t steps, valid, emit;        // RK4 steps traced, valid samples, emitting segments integrated
+    int32_t trace_status;              // -1 while the geodesic is traced, then its BHN_RAY_* end
+    int32_t status;                    // -1 until the ray's result is written
+    int32_t count;                     // emitting segments listed in this round
+};
+
+struct SegIn {    // one emitting segment's plasma frame (the coefficient kernel's input)
+    double n_e, te, b, cos_los, chi, nu_emit, jf, kf;
+};
+struct SegSide {  // what the transfer needs besides the coefficients
+    double ds, g;
+    int32_t step, valid;
+};
+
+struct WaveState {
+    GrrtRay *ray;               // [rays]
+    SegIn *seg;                 // [rays * chunk], in append order
+    SegSide *side;              // [rays][chunk]
+    int32_t *slot;              // [rays][chunk]: index of the ray's k-th segment in seg / coef
+    double *coef;               // [rays * chunk][12]: scaled coefficients
+    unsigned long long *n_seg;  // segments listed in this round
+    int64_t rays;
+    int32_t chunk;
+};
+
+struct TraceParams {
     const double *fields;       // [nr][nt][np][11]: rho, Theta_e, pressure, b^mu (4), u^mu (4)
     const double *rg, *tg, *pg;
-    int nr, nt, np;
+    int nr, nt, np, max_steps;
     const ViewDev *view;
-    double step, escape_radius, nu, length_cm, max_tau, min_redshift, flux_scale;
-    int max_steps, exact_step;
+    double step, escape_radius, nu, length_cm, min_redshift, flux_scale, rho_unit, b_unit, mu_e_mp;
+    WaveState W;
+};
+struct CoefParams {
+    synch::Model M;
+    WaveState W;
+};
+struct TransferParams {
+    const ViewDev *view;
+    double max_tau;
+    int exact_step;
     double *out;                // [rays][4] Stokes
     double *diag;               // optional [rays][8]: tau, emit, valid, faraday depth, g min, g max, steps, status
-    unsigned long long *queue;  // next ray to hand out (zeroed before the launch)
+    WaveState W;
 };
 
 __device__ __forceinline__ void rk4_state(const double y[5], double h, double a, double pt, double pphi, double yn[5]) {
@@ -52,149 +97,229 @@ __device__ __forceinline__ void rk4_state(const double y[5], double h, double a,
     yn[4] = y[4] + h6 * (((k1.pth + 2.0 * k2.pth) + 2.0 * k3.pth) + k4.pth);
 }
 
-// The state a ray carries across its segments, one copy per warp in shared
-// memory: the lanes hold identical values (they run the same arithmetic, and
-// the butterfly sums of the coefficient integrals give every lane the same
-// bits), so every lane stores and reloads the same numbers.  Keeping it out of
-// registers while the warp evaluates a segment's synchrotron integrals leaves
-// those registers to the integrals.
-struct RayState {
-    double y[5], S[4], tau, fd, gmin, gmax, prev_r, pt, pphi;
-};
-
-__global__ void __launch_bounds__(128, 4) grrt_kernel(const __grid_constant__ GrrtParams P) {
-    __shared__ synch::TableSmem T;
-    __shared__ RayState ray_state[4];
-    synch::load_table(T, P.M);
-    __syncthreads();
-    const ViewDev &v = *P.view;
-    const int lane = threadIdx.x & 31;
-    volatile RayState &st = ray_state[threadIdx.x >> 5];
-    const int64_t rays = (int64_t)v.crop_w * v.crop_h;
-    // Rays differ by orders of magnitude in emitting segments: a persistent
-    // grid whose warps take the next ray from one counter keeps every warp busy
-    // until the last rays.
-    for (;;) {
-        unsigned long long next = 0;
-        if (lane == 0) next = atomicAdd(P.queue, 1ull);
-        const int64_t ray = (int64_t)__shfl_sync(0xffffffffu, next, 0);
-        if (ray >= rays) break;
-        const int px = v.x0 + (int)(ray % v.crop_w), py = v.y0 + (int)(ray / v.crop_w);
-        {
-            const CameraRay cam = camera_ray(v, px, py);
-            st.y[0] = v.r_obs;
-            st.y[1] = v.theta_obs;
-            st.y[2] = v.phi_obs;
-            st.y[3] = cam.pr;
-            st.y[4] = cam.pth;
-            st.pt = cam.pt;
-            st.pphi = cam.pphi;
-            for (int k = 0; k < 4; ++k) st.S[k] = 0.0;
-            st.tau = 0.0;
-            st.fd = 0.0;
-            st.gmin = INFINITY;
-            st.gmax = 0.0;
-            st.prev_r = v.r_obs;
-        }
-        int emit = 0, valid = 0, steps = 0, status = v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID;
-        for (int i = 1; i <= P.max_steps && v.valid; ++i) {
-            const double a = v.a, pt = st.pt, pphi = st.pphi;
-            double y[5], yn[5];
-            for (int k = 0; k < 5; ++k) y[k] = st.y[k];
-            rk4_state(y, P.step, a, pt, pphi, yn);
-            steps = i;
-            if (!(isfinite(yn[0]) && isfinite(yn[1]) && isfinite(yn[2]) && isfinite(yn[3]) && isfinite(yn[4]))) {
-                status = BHN_RAY_INVALID;  // kerr.py:364-366: not stored, no segment
-                break;
-            }
-            for (int k = 0; k < 5; ++k) st.y[k] = yn[k];
-            // segment (y, yn): polarized_transfer.py:103-143
-            const double mr = 0.5 * (y[0] + yn[0]), mth = 0.5 * (y[1] + yn[1]), mph = 0.5 * (y[2] + yn[2]);
-            const double mpr = 0.5 * (y[3] + yn[3]), mpth = 0.5 * (y[4] + yn[4]);
-            double f[11];
-            const bool inside = isfinite(mr) && isfinite(mth) && isfinite(mph) &&
-                                sample_one_exact(P.fields, P.rg, P.nr, P.tg, P.nt, P.pg, P.np, mr, mth, mph, f);
-            // grmhd.py:119-120: rho > 0, Theta_e > 0, finite u
-            if (inside && f[0] > 0.0 && f[1] > 0.0 && isfinite(f[7]) && isfinite(f[8]) && isfinite(f[9]) &&
-                isfinite(f[10])) {
-                ++valid;
-                // radiative_transfer.py:91-99
-                const double e_emit = -(((pt * f[7] + mpr * f[8]) + mpth * f[9]) + pphi * f[10]);
-                const double g = (e_emit > 0.0 && isfinite(e_emit)) ? 1.0 / e_emit : 0.0;
-                if (g >= P.min_redshift) {
-                    // synchrotron.py:104-117 with calibration.py:113-119
-                    const double b1 = f[4], b2 = f[5], b3 = f[6];
-                    const double b_code = sqrt((b1 * b1 + b2 * b2) + b3 * b3);
-                    const double n_e = f[0] * P.M.rho_unit / P.M.mu_e_mp;
-                    double cos_los = 0.0;
-                    if (b_code > 0.0) {
-                        const double nk = sqrt((mpr * mpr + mpth * mpth) + pphi * pphi);
-                        if (nk > 0.0)
-                            cos_los = fmin(fmax(((b1 * mpr + b2 * mpth) + b3 * pphi) / (b_code * nk), -1.0), 1.0);
-                    }
-                    const double chi = b_code > 0.0 ? atan2(b3, b2) : 0.0;
-                    const double te = fmax(f[1], 1.0e-8), b = fmax(b_code * P.M.b_unit, 0.0);
-                    const double jf = g * g * P.flux_scale, kf = 1.0 / fmax(g, 1.0e-300);
-                    const double dr = yn[0] - y[0], dth = yn[1] - y[1], dph = yn[2] - y[2];
-                    const double dl = sqrt((dr * dr + dth * dth) + dph * dph);
-                    const double ds = P.length_cm * fmax(e_emit, 0.0) * fmax(dl, 1.0e-14);
-                    st.gmin = fmin(st.gmin, g);
-                    st.gmax = fmax(st.gmax, g);
-                    double c[11];
-                    synch::coefficients(T, P.M, n_e, te, b, cos_los, chi, P.nu / g, c);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) c[k] *= jf;
-#pragma unroll
-                    for (int k = 4; k < 11; ++k) c[k] *= kf;
-                    double S[4];
-                    for (int k = 0; k < 4; ++k) S[k] = st.S[k];
-                    if (P.exact_step)
-                        stokes_step_exact(S, c, ds);
-                    else
-                        stokes_step_rk2_exact(S, c, ds);
-                    for (int k = 0; k < 4; ++k) st.S[k] = S[k];
-                    const double tau = st.tau + fmax(c[4], 0.0) * ds;
-                    st.tau = tau;
-                    st.fd = st.fd + (fabs(c[8]) + fabs(c[9]) + fabs(c[10])) * ds;
-                    ++emit;
-                    if (tau >= P.max_tau) {
-                        status = BHN_RAY_OPAQUE;
-                        break;
-                    }
-                }
-            }
-            // kerr.py:370-378
-            const double r = st.y[0];
-            if (r <= v.r_capture) {
-                status = BHN_RAY_CAPTURED;
-                break;
-            }
-            if (r > P.escape_radius && r > st.prev_r) {
-                status = BHN_RAY_ESCAPED;
-                break;
-            }
-            st.prev_r = r;
-        }
-        if (lane == 0) {
-            const int64_t o = v.out_offset + (int64_t)(py - v.y0) * v.crop_w + (px - v.x0);
-            for (int k = 0; k < 4; ++k) P.out[4 * o + k] = st.S[k];
-            if (P.diag) {
-                double *d = P.diag + 8 * o;
-                d[0] = st.tau;
-                d[1] = emit;
-                d[2] = valid;
-                d[3] = st.fd;
-                d[4] = st.gmin < INFINITY ? st.gmin : 0.0;
-                d[5] = st.gmax;
-                d[6] = steps;
-                d[7] = status;
-            }
-        }
-        __syncwarp();  // every lane is done with this ray's state before the next ray overwrites it
+__device__ __forceinline__ void write_result(const ViewDev &v, int64_t ray, const GrrtRay &R, int status,
+                                             double *out, double *diag) {
+    const int64_t o = v.out_offset + ray;  // the crop's rays in row order
+    for (int k = 0; k < 4; ++k) out[4 * o + k] = R.S[k];
+    if (diag) {
+        double *d = diag + 8 * o;
+        d[0] = R.tau;
+        d[1] = R.emit;
+        d[2] = R.valid;
+        d[3] = R.fd;
+        d[4] = R.gmin < INFINITY ? R.gmin : 0.0;
+        d[5] = R.gmax;
+        d[6] = R.steps;
+        d[7] = status;
     }
 }
 
+__global__ void __launch_bounds__(128) grrt_init_kernel(const TraceParams P, double *out, double *diag) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= P.W.rays) return;
+    const ViewDev &v = *P.view;
+    GrrtRay &R = P.W.ray[r];
+    const int px = v.x0 + (int)(r % v.crop_w), py = v.y0 + (int)(r / v.crop_w);
+    const CameraRay cam = camera_ray(v, px, py);
+    R.y[0] = v.r_obs;
+    R.y[1] = v.theta_obs;
+    R.y[2] = v.phi_obs;
+    R.y[3] = cam.pr;
+    R.y[4] = cam.pth;
+    R.pt = cam.pt;
+    R.pphi = cam.pphi;
+    R.prev_r = v.r_obs;
+    for (int k = 0; k < 4; ++k) R.S[k] = 0.0;
+    R.tau = R.fd = R.gmax = 0.0;
+    R.gmin = INFINITY;
+    R.steps = R.valid = R.emit = R.count = 0;
+    R.trace_status = -1;
+    R.status = -1;
+    if (!v.valid) {
+        R.status = BHN_RAY_INVALID;
+        write_result(v, r, R, BHN_RAY_INVALID, out, diag);
+    }
+}
+
+__global__ void __launch_bounds__(128) grrt_trace_kernel(const TraceParams P) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= P.W.rays) return;
+    GrrtRay &R = P.W.ray[r];
+    R.count = 0;
+    if (R.status >= 0 || R.trace_status >= 0) return;
+    const ViewDev &v = *P.view;
+    const double a = v.a, pt = R.pt, pphi = R.pphi;
+    double y[5] = {R.y[0], R.y[1], R.y[2], R.y[3], R.y[4]};
+    double prev_r = R.prev_r;
+    int steps = R.steps, valid = R.valid, count = 0, ts = -1;
+    SegSide *side = P.W.side + r * P.W.chunk;
+    int32_t *slot = P.W.slot + r * P.W.chunk;
+    for (;;) {
+        if (steps >= P.max_steps) {
+            ts = BHN_RAY_MAX_STEPS;
+            break;
+        }
+        double yn[5];
+        rk4_state(y, P.step, a, pt, pphi, yn);
+        ++steps;
+        if (!(isfinite(yn[0]) && isfinite(yn[1]) && isfinite(yn[2]) && isfinite(yn[3]) && isfinite(yn[4]))) {
+            ts = BHN_RAY_INVALID;  // kerr.py:364-366: not stored, no segment
+            break;
+        }
+        // segment (y, yn): polarized_transfer.py:103-143
+        const double mr = 0.5 * (y[0] + yn[0]), mth = 0.5 * (y[1] + yn[1]), mph = 0.5 * (y[2] + yn[2]);
+        const double mpr = 0.5 * (y[3] + yn[3]), mpth = 0.5 * (y[4] + yn[4]);
+        double f[11];
+        const bool inside = isfinite(mr) && isfinite(mth) && isfinite(mph) &&
+                            sample_one_exact(P.fields, P.rg, P.nr, P.tg, P.nt, P.pg, P.np, mr, mth, mph, f);
+        // grmhd.py:119-120: rho > 0, Theta_e > 0, finite u
+        if (inside && f[0] > 0.0 && f[1] > 0.0 && isfinite(f[7]) && isfinite(f[8]) && isfinite(f[9]) &&
+            isfinite(f[10])) {
+            ++valid;
+            // radiative_transfer.py:91-99
+            const double e_emit = -(((pt * f[7] + mpr * f[8]) + mpth * f[9]) + pphi * f[10]);
+            const double g = (e_emit > 0.0 && isfinite(e_emit)) ? 1.0 / e_emit : 0.0;
+            if (g >= P.min_redshift) {
+                // synchrotron.py:104-117 with calibration.py:113-119
+                const double b1 = f[4], b2 = f[5], b3 = f[6];
+                const double b_code = sqrt((b1 * b1 + b2 * b2) + b3 * b3);
+                SegIn s;
+                s.n_e = f[0] * P.rho_unit / P.mu_e_mp;
+                s.cos_los = 0.0;
+                if (b_code > 0.0) {
+                    const double nk = sqrt((mpr * mpr + mpth * mpth) + pphi * pphi);
+                    if (nk > 0.0)
+                        s.cos_los = fmin(fmax(((b1 * mpr + b2 * mpth) + b3 * pphi) / (b_code * nk), -1.0), 1.0);
+                }
+                s.chi = b_code > 0.0 ? atan2(b3, b2) : 0.0;
+                s.te = fmax(f[1], 1.0e-8);
+                s.b = fmax(b_code * P.b_unit, 0.0);
+                s.nu_emit = P.nu / g;
+                s.jf = g * g * P.flux_scale;
+                s.kf = 1.0 / fmax(g, 1.0e-300);
+                const double dr = yn[0] - y[0], dth = yn[1] - y[1], dph = yn[2] - y[2];
+                const double dl = sqrt((dr * dr + dth * dth) + dph * dph);
+                SegSide sd;
+                sd.ds = P.length_cm * fmax(e_emit, 0.0) * fmax(dl, 1.0e-14);
+                sd.g = g;
+                sd.step = steps;
+                sd.valid = valid;
+                const unsigned long long idx = atomicAdd(P.W.n_seg, 1ull);
+                P.W.seg[idx] = s;
+                side[count] = sd;
+                slot[count] = (int32_t)idx;
+                ++count;
+            }
+        }
+        for (int k = 0; k < 5; ++k) y[k] = yn[k];
+        // kerr.py:370-378
+        if (y[0] <= v.r_capture) {
+            ts = BHN_RAY_CAPTURED;
+            break;
+        }
+        if (y[0] > P.escape_radius && y[0] > prev_r) {
+            ts = BHN_RAY_ESCAPED;
+            break;
+        }
+        prev_r = y[0];
+        if (count == P.W.chunk) break;  // this round's list is full: continue in the next round
+    }
+    for (int k = 0; k < 5; ++k) R.y[k] = y[k];
+    R.prev_r = prev_r;
+    R.steps = steps;
+    R.valid = valid;
+    R.count = count;
+    R.trace_status = ts;
+}
+
+// One warp per listed segment (a persistent grid over this round's list).
+__global__ void __launch_bounds__(128, 6) grrt_coef_kernel(const __grid_constant__ CoefParams P) {
+    __shared__ synch::TableSmem T;
+    synch::load_table(T, P.M);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const unsigned long long n = *P.W.n_seg;
+    const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+    for (unsigned long long i = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const SegIn s = P.W.seg[i];
+        double c[11];
+        synch::coefficients(T, P.M, s.n_e, s.te, s.b, s.cos_los, s.chi, s.nu_emit, c);
+        double *o = P.W.coef + 12 * i;
+#pragma unroll
+        for (int k = 0; k < 11; ++k)
+            if (lane == k) o[k] = c[k] * (k < 4 ? s.jf : s.kf);
+    }
+}
+
+__global__ void __launch_bounds__(128) grrt_transfer_kernel(const TransferParams P) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *P.W.n_seg = 0;  // the coefficient kernel has read it
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= P.W.rays) return;
+    GrrtRay &R = P.W.ray[r];
+    if (R.status >= 0) return;
+    const SegSide *side = P.W.side + r * P.W.chunk;
+    const int32_t *slot = P.W.slot + r * P.W.chunk;
+    double S[4] = {R.S[0], R.S[1], R.S[2], R.S[3]};
+    double tau = R.tau, fd = R.fd, gmin = R.gmin, gmax = R.gmax;
+    int emit = R.emit, status = -1;
+    for (int k = 0; k < R.count; ++k) {
+        const SegSide sd = side[k];
+        const double *cp = P.W.coef + 12 * (int64_t)slot[k];
+        double c[11];
+        for (int q = 0; q < 11; ++q) c[q] = cp[q];
+        if (P.exact_step)
+            stokes_step_exact(S, c, sd.ds);
+        else
+            stokes_step_rk2_exact(S, c, sd.ds);
+        tau = tau + fmax(c[4], 0.0) * sd.ds;
+        fd = fd + (fabs(c[8]) + fabs(c[9]) + fabs(c[10])) * sd.ds;
+        ++emit;
+        gmin = fmin(gmin, sd.g);
+        gmax = fmax(gmax, sd.g);
+        if (tau >= P.max_tau) {  // polarized_transfer.py:141-142: the ray ends at this segment
+            status = BHN_RAY_OPAQUE;
+            R.steps = sd.step;
+            R.valid = sd.valid;
+            break;
+        }
+    }
+    for (int q = 0; q < 4; ++q) R.S[q] = S[q];
+    R.tau = tau;
+    R.fd = fd;
+    R.gmin = gmin;
+    R.gmax = gmax;
+    R.emit = emit;
+    if (status < 0) status = R.trace_status;
+    if (status >= 0) {
+        R.status = status;
+        write_result(*P.view, r, R, status, P.out, P.diag);
+    }
+}
+
+struct GrrtLayout {
+    int64_t views, n_seg, ray, seg, side, slot, coef, total;
+};
+inline GrrtLayout grrt_layout(int64_t rays, int64_t chunk) {
+    auto up = [](int64_t x) { return (x + 255) & ~(int64_t)255; };
+    GrrtLayout L;
+    L.views = 0;
+    L.n_seg = up(scratch_layout(1).total);
+    L.ray = L.n_seg + 256;
+    L.seg = up(L.ray + rays * (int64_t)sizeof(GrrtRay));
+    L.side = up(L.seg + rays * chunk * (int64_t)sizeof(SegIn));
+    L.slot = up(L.side + rays * chunk * (int64_t)sizeof(SegSide));
+    L.coef = up(L.slot + rays * chunk * 4);
+    L.total = up(L.coef + rays * chunk * 12 * 8);
+    return L;
+}
+constexpr int64_t kGrrtMaxChunk = 4096;
+
 }  // namespace bhn
+
+extern "C" int64_t bhn_grrt_scratch_bytes(int64_t rays, int32_t chunk) {
+    if (rays < 0 || chunk < 1) return -1;
+    return bhn::grrt_layout(rays, chunk).total;
+}
 
 extern "C" int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, const double *theta_grid,
                                int32_t nt, const double *phi_grid, int32_t np, const bhn_view *view,
@@ -209,44 +334,88 @@ extern "C" int bhn_grrt_render(const double *fields, const double *r_grid, int32
     if (!(cfg->nu_hz > 0.0) || !std::isfinite(cfg->nu_hz)) return fail(BHN_ERR_VALUE, "observing frequency must be positive");
     if (!(cfg->length_cm > 0.0) || !std::isfinite(cfg->length_cm))
         return fail(BHN_ERR_VALUE, "affine-to-length scale must be finite and positive");
-    static GrrtParams P;  // ~10 KB: kept off the host stack; filled under the lock
-    static std::mutex lock;
-    std::lock_guard<std::mutex> g(lock);
-    int rc = synch::fill_model(model, P.M);
-    if (rc) return rc;
-    rc = bhn_render_prepare(view, 1, scratch, scratch_bytes, stream);  // FP64 camera tables of the view
-    if (rc) return rc;
-    const ScratchLayout L = scratch_layout(1);
-    unsigned char *sc = reinterpret_cast<unsigned char *>(scratch);
-    P.fields = fields;
-    P.rg = r_grid;
-    P.tg = theta_grid;
-    P.pg = phi_grid;
-    P.nr = nr;
-    P.nt = nt;
-    P.np = np;
-    P.view = reinterpret_cast<const ViewDev *>(sc + L.views);
-    P.step = cfg->step;
-    P.escape_radius = cfg->escape_radius;
-    P.nu = cfg->nu_hz;
-    P.length_cm = cfg->length_cm;
-    P.max_tau = cfg->max_optical_depth;
-    P.min_redshift = cfg->min_redshift;
-    P.flux_scale = cfg->flux_scale;
-    P.max_steps = cfg->max_steps;
-    P.exact_step = cfg->exact_step != 0;
-    P.out = out;
-    P.diag = diag;
     const int64_t rays = (int64_t)view->crop_w * view->crop_h;
     if (rays <= 0) return BHN_OK;
+    // the largest chunk the scratch holds
+    int64_t chunk = 0;
+    for (int64_t lo = 1, hi = kGrrtMaxChunk; lo <= hi;) {
+        const int64_t mid = (lo + hi) / 2;
+        if (grrt_layout(rays, mid).total <= scratch_bytes) {
+            chunk = mid;
+            lo = mid + 1;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    if (chunk < 1)
+        return fail(BHN_ERR_VALUE, "scratch too small: bhn_grrt_scratch_bytes(rays, 1) = " +
+                                       std::to_string(grrt_layout(rays, 1).total) + " bytes");
+    static CoefParams C;  // ~10 KB (the model's tables): kept off the host stack; filled under the lock
+    static std::mutex lock;
+    std::lock_guard<std::mutex> g(lock);
+    int rc = synch::fill_model(model, C.M);
+    if (rc) return rc;
+    rc = bhn_render_prepare(view, 1, scratch, scratch_layout(1).total, stream);  // FP64 camera tables of the view
+    if (rc) return rc;
+    const GrrtLayout GL = grrt_layout(rays, chunk);
+    unsigned char *sc = reinterpret_cast<unsigned char *>(scratch);
+    WaveState W;
+    W.ray = reinterpret_cast<GrrtRay *>(sc + GL.ray);
+    W.seg = reinterpret_cast<SegIn *>(sc + GL.seg);
+    W.side = reinterpret_cast<SegSide *>(sc + GL.side);
+    W.slot = reinterpret_cast<int32_t *>(sc + GL.slot);
+    W.coef = reinterpret_cast<double *>(sc + GL.coef);
+    W.n_seg = reinterpret_cast<unsigned long long *>(sc + GL.n_seg);
+    W.rays = rays;
+    W.chunk = (int32_t)chunk;
+    C.W = W;
+    const ViewDev *vd = reinterpret_cast<const ViewDev *>(sc + scratch_layout(1).views);
+    TraceParams T;
+    T.fields = fields;
+    T.rg = r_grid;
+    T.tg = theta_grid;
+    T.pg = phi_grid;
+    T.nr = nr;
+    T.nt = nt;
+    T.np = np;
+    T.max_steps = cfg->max_steps;
+    T.view = vd;
+    T.step = cfg->step;
+    T.escape_radius = cfg->escape_radius;
+    T.nu = cfg->nu_hz;
+    T.length_cm = cfg->length_cm;
+    T.min_redshift = cfg->min_redshift;
+    T.flux_scale = cfg->flux_scale;
+    T.rho_unit = C.M.rho_unit;
+    T.b_unit = C.M.b_unit;
+    T.mu_e_mp = C.M.mu_e_mp;
+    T.W = W;
+    TransferParams X;
+    X.view = vd;
+    X.max_tau = cfg->max_optical_depth;
+    X.exact_step = cfg->exact_step != 0;
+    X.out = out;
+    X.diag = diag;
+    X.W = W;
     int dev = 0, sms = 148, per_sm = 0;
     BHN_CUDA_TRY(cudaGetDevice(&dev));
     BHN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    BHN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grrt_kernel, 128, 0));
-    const int64_t blocks = std::min<int64_t>((rays + 3) / 4, (int64_t)sms * std::max(per_sm, 1));
-    P.queue = reinterpret_cast<unsigned long long *>(sc + L.queue);
-    BHN_CUDA_TRY(cudaMemsetAsync(P.queue, 0, sizeof(unsigned long long), as_stream(stream)));
-    grrt_kernel<<<(unsigned)blocks, 128, 0, as_stream(stream)>>>(P);
-    BHN_LAUNCH_CHECK("grrt_kernel");
+    BHN_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grrt_coef_kernel, 128, 0));
+    cudaStream_t s = as_stream(stream);
+    const unsigned ray_blocks = (unsigned)((rays + 127) / 128);
+    const unsigned coef_blocks = (unsigned)std::min<int64_t>((rays * chunk + 3) / 4, (int64_t)sms * std::max(per_sm, 1));
+    BHN_CUDA_TRY(cudaMemsetAsync(W.n_seg, 0, sizeof(unsigned long long), s));
+    grrt_init_kernel<<<ray_blocks, 128, 0, s>>>(T, out, diag);
+    BHN_LAUNCH_CHECK("grrt_init_kernel");
+    // every round either ends a ray's trace or lists chunk segments of it, one step each at least
+    const int64_t rounds = (int64_t)cfg->max_steps / chunk + 2;
+    for (int64_t k = 0; k < rounds; ++k) {
+        grrt_trace_kernel<<<ray_blocks, 128, 0, s>>>(T);
+        BHN_LAUNCH_CHECK("grrt_trace_kernel");
+        grrt_coef_kernel<<<coef_blocks, 128, 0, s>>>(C);
+        BHN_LAUNCH_CHECK("grrt_coef_kernel");
+        grrt_transfer_kernel<<<ray_blocks, 128, 0, s>>>(X);
+        BHN_LAUNCH_CHECK("grrt_transfer_kernel");
+    }
     return BHN_OK;
 }

@@ -111,7 +111,7 @@ struct Integrals {
 // distribution, split over the warp's lanes.  thermal: f = gamma^2 beta
 // exp(-gamma / theta_e) on 1 + geomspace(1e-5, gmax - 1); power law: f =
 // gamma^-p on geomspace(gamma_min, gamma_max).
-__device__ inline Integrals integrate(const TableSmem &T, const Component &C, bool thermal, double theta_e, double base) {
+static __device__ __noinline__ Integrals integrate(const TableSmem &T, const Component &C, bool thermal, double theta_e, double base) {
     const int n = C.gamma_n, lane = threadIdx.x & 31;
     double g0, g1;
     if (thermal) {

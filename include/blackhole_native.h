@@ -339,7 +339,10 @@ int bhn_brick_precompute(const double *rho, const double *theta_e, const double 
  * snapshot (grmhd.py:55-121); out: [rays][4] Stokes of the view's crop in row
  * order (at view->out_offset); diag (optional): [rays][8] = optical depth,
  * emitting segments, valid segments, Faraday depth, min / max redshift,
- * steps traced, BHN_RAY_* status.  scratch: bhn_render_scratch_bytes(1). */
+ * steps traced, BHN_RAY_* status.  scratch: bhn_grrt_scratch_bytes(rays,
+ * chunk) bytes, 256-byte aligned; the renderer lists up to `chunk` emitting
+ * segments per ray and round (the largest chunk the scratch holds, <= 4096),
+ * so a larger scratch means fewer rounds.  Results do not depend on it. */
 typedef struct bhn_grrt_config {
     double step;                 /* affine RK4 step (PolarizedRenderConfig.step) */
     double escape_radius;
@@ -349,6 +352,7 @@ typedef struct bhn_grrt_config {
     int32_t max_steps;
     int32_t exact_step;          /* 1: stokes_step_exact, 0: RK2 (PolarizedTransferConfig.use_exact_matrix_step) */
 } bhn_grrt_config;
+int64_t bhn_grrt_scratch_bytes(int64_t rays, int32_t chunk);
 int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, const double *theta_grid, int32_t nt,
                     const double *phi_grid, int32_t np, const bhn_view *view, const bhn_synchrotron_model *model,
                     const bhn_grrt_config *cfg, void *scratch, int64_t scratch_bytes, double *out, double *diag,

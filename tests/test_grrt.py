@@ -145,3 +145,27 @@ def test_gpu_seeded_snapshot_device_reuse_against_oracle():
         S, _ = G.trace_pixel(v, grrt.snapshot_fields(snap), snap.r, snap.theta, snap.phi, sc, 230e9, 0.1, 900, 220.0,
                              length_cm=scaling.rg_cm, exact=False, px=px, py=py)
         assert _rel(host[py, px], S) <= 1e-10 if np.any(S) else not np.any(host[py, px])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("exact", [False, True])
+def test_gpu_chunk_does_not_change_the_image(golden, exact):
+    """The renderer lists `chunk` emitting segments per ray and round; one
+    segment per round, three, and the default give the same image and
+    diagnostics bit for bit (a tiny optical-depth cutoff makes rays end
+    mid-round, after segments their trace already listed)."""
+    from blackhole_native import grrt
+
+    cam = golden["cam"]
+    snap, sc = _snapshot(golden), _scaling(golden)
+    for max_tau in (30.0, 1e-6):
+        tr = grrt.PolarizedTransferConfig(use_exact_matrix_step=exact, max_optical_depth=max_tau)
+        cfg = grrt.PolarizedRenderConfig(width=12, height=8, camera=grrt.LocalCamera(*cam), step=0.1, max_steps=900,
+                                         transfer=tr)
+        ref, ref_d = (t.cpu().numpy() for t in grrt.render_stokes_image_device(cfg, snap, sc, diagnostics=True))
+        if max_tau < 1.0:
+            assert np.any(ref_d[..., 7] == 4)  # some rays end opaque
+        for chunk in (1, 3):
+            img, d = (t.cpu().numpy() for t in grrt.render_stokes_image_device(cfg, snap, sc, diagnostics=True,
+                                                                             chunk=chunk))
+            assert np.array_equal(img, ref) and np.array_equal(d, ref_d), (max_tau, chunk)
