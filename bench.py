@@ -511,15 +511,16 @@ def fp64_peaks(device, stream) -> dict:
 
 
 def exps_per_evaluation(model_struct) -> int:
-    """Double exp() calls of the kernel-table lookups in one coefficient
-    evaluation: F and G at every (Lorentz-factor node, pitch node) pair of
-    each component."""
+    """Double exp() calls of the kernel-table lookups one coefficient
+    evaluation needs: F and G at every Lorentz-factor node and distinct pitch
+    angle of each component (the Gauss-Legendre nodes +-mu share sin(alpha),
+    so an n-node rule has (n + 1) // 2 distinct angles)."""
     m = model_struct
     n = 0
     if m.thermal:
-        n += m.thermal_gamma_n * m.thermal_pitch_n
+        n += m.thermal_gamma_n * ((m.thermal_pitch_n + 1) // 2)
     if m.nonthermal:
-        n += m.nonthermal_gamma_n * m.nonthermal_pitch_n
+        n += m.nonthermal_gamma_n * ((m.nonthermal_pitch_n + 1) // 2)
     return 2 * n
 
 

@@ -163,9 +163,19 @@ void pitch_set(int n, PitchSet &ps) {
     for (int m = 0; m < n; ++m) {
         const double sin_a = std::sqrt(std::max(0.0, 1.0 - x[m] * x[m]));
         if (!(sin_a > 0.0)) continue;  // Bp = B sin(alpha) <= 0 contributes nothing
-        ps.log_sin[ps.n] = std::log(sin_a);
-        ps.log_sin_max = ps.n == 0 ? ps.log_sin[0] : std::max(ps.log_sin_max, ps.log_sin[ps.n]);
-        ps.weight[ps.n] = 0.5 * w[m] * pref * sin_a;
+        const double ls = std::log(sin_a), wt = 0.5 * w[m] * pref * sin_a;
+        // the Gauss-Legendre nodes come in pairs +-mu with one sin(alpha) and one
+        // weight: the pair's two lookups are the same numbers, so it is one node
+        // of twice the weight
+        int k = 0;
+        while (k < ps.n && ps.log_sin[k] != ls) ++k;
+        if (k < ps.n) {
+            ps.weight[k] += wt;
+            continue;
+        }
+        ps.log_sin[ps.n] = ls;
+        ps.log_sin_max = ps.n == 0 ? ls : std::max(ps.log_sin_max, ls);
+        ps.weight[ps.n] = wt;
         ++ps.n;
     }
 }
