@@ -64,10 +64,17 @@ struct Model {
     Component th, nt;
 };
 
+constexpr int kNodeCache = 256;  // power-law nodes kept per block (the default grid has 224)
+
 struct TableSmem {
     double lx[kTable], lF[kTable], lG[kTable], sF[kTable], sG[kTable];
     double inv;      // (kTable - 1) / (lx[last] - lx[0]): knots per unit of log x
     double lx_tail;  // Model::lx_tail
+    // The power law's nodes do not depend on the cell: its trapezoid weights
+    // times gamma^-p and 2 log gamma, computed once per block (when it has at
+    // most kNodeCache nodes), exactly as integrate() would per evaluation.
+    int nt_cached;
+    double nt_w[kNodeCache], nt_lg[kNodeCache];
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -107,6 +114,27 @@ struct Integrals {
     double norm, I, Q;   // sum c_i f_i, sum c_i f_i sum_m W_m F, sum c_i f_i sum_m W_m G
 };
 
+// One node's pitch sums: W_m F(x_m), W_m G(x_m) over the distinct pitch angles,
+// x_m = nu / (1.5 nu_B sin(alpha_m) gamma^2) as log x = base - log sin - 2 log gamma.
+// A node whose smallest x (the pitch with the largest sin) already lies in
+// the table's far tail adds terms below kTailValue times the pitch weights
+// (< 1e-270): nothing a cell that emits can resolve.  Skipping it leaves such
+// cells unchanged to the last bit (one that does not emit at all gets 0
+// instead of a sum of those terms).
+__device__ __forceinline__ void pitch_sums(const TableSmem &T, const PitchSet &ps, double base, double two_lg,
+                                           double w, Integrals &acc) {
+    if (!(w != 0.0 && __dsub_rn(__dsub_rn(base, ps.log_sin_max), two_lg) < T.lx_tail)) return;
+    double sI = 0.0, sQ = 0.0;
+    for (int m = 0; m < ps.n; ++m) {
+        double F, G;
+        kernel_lookup(T, base - ps.log_sin[m] - two_lg, F, G);
+        sI = fma(ps.weight[m], F, sI);
+        sQ = fma(ps.weight[m], G, sQ);
+    }
+    acc.I += w * sI;
+    acc.Q += w * sQ;
+}
+
 // The pitch-averaged trapezoid integrals of synchrotron.py:207-237 for one
 // distribution, split over the warp's lanes.  thermal: f = gamma^2 beta
 // exp(-gamma / theta_e) on 1 + geomspace(1e-5, gmax - 1); power law: f =
@@ -124,6 +152,17 @@ static __device__ __noinline__ Integrals integrate(const TableSmem &T, const Com
     const double ls = log10(g0), step = (log10(g1) - ls) / (double)(n - 1);
     const double inv_te = 1.0 / fmax(theta_e, 1.0e-12);
     Integrals acc = {0.0, 0.0, 0.0};
+    if (!thermal && T.nt_cached) {
+        for (int i = lane; i < n; i += 32) {
+            const double w = T.nt_w[i];
+            acc.norm += w;
+            pitch_sums(T, C.pitch, base, T.nt_lg[i], w, acc);
+        }
+        acc.norm = warp_sum(acc.norm);
+        acc.I = warp_sum(acc.I);
+        acc.Q = warp_sum(acc.Q);
+        return acc;
+    }
     // Each lane evaluates one node per chunk of 32 (the next chunk's one step
     // ahead); the trapezoid's neighbours come from the adjacent lanes.
     double x_cur = geom_node(g0, g1, ls, step, lane, n), x_last = 0.0;
@@ -159,23 +198,7 @@ static __device__ __noinline__ Integrals integrate(const TableSmem &T, const Com
         }
         const double w = c * f;
         acc.norm += w;
-        const double two_lg = w != 0.0 ? 2.0 * log(gamma) : 0.0;
-        // A node whose smallest x (the pitch with the largest sin) already lies
-        // in the table's far tail adds terms below kTailValue times the pitch
-        // weights (< 1e-270): nothing a cell that emits can resolve.  Skipping
-        // it leaves such cells unchanged to the last bit (one that does not
-        // emit at all gets 0 instead of a sum of those terms).
-        if (w != 0.0 && __dsub_rn(__dsub_rn(base, C.pitch.log_sin_max), two_lg) < T.lx_tail) {
-            double sI = 0.0, sQ = 0.0;
-            for (int m = 0; m < C.pitch.n; ++m) {
-                double F, G;
-                kernel_lookup(T, base - C.pitch.log_sin[m] - two_lg, F, G);
-                sI = fma(C.pitch.weight[m], F, sI);
-                sQ = fma(C.pitch.weight[m], G, sQ);
-            }
-            acc.I += w * sI;
-            acc.Q += w * sQ;
-        }
+        pitch_sums(T, C.pitch, base, w != 0.0 ? 2.0 * log(gamma) : 0.0, w, acc);
     }
     acc.norm = warp_sum(acc.norm);
     acc.I = warp_sum(acc.I);
@@ -222,6 +245,24 @@ __device__ __forceinline__ void load_table(TableSmem &T, const Model &M) {
     if (threadIdx.x == 0) {
         T.inv = (double)(kTable - 1) / (M.lx[kTable - 1] - M.lx[0]);
         T.lx_tail = M.lx_tail;
+    }
+    // the power law's nodes (integrate()'s arithmetic for them, once)
+    const Component &C = M.nt;
+    const bool cache = C.on && C.gamma_n <= kNodeCache;
+    if (threadIdx.x == 0) T.nt_cached = cache;
+    if (!cache) return;
+    const int n = C.gamma_n;
+    const double g0 = C.gamma_min, g1 = C.gamma_max;
+    const double ls = log10(g0), step = (log10(g1) - ls) / (double)(n - 1);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double xi = geom_node(g0, g1, ls, step, i, n);
+        const double xm = i > 0 ? geom_node(g0, g1, ls, step, i - 1, n) : xi;
+        const double xp = i < n - 1 ? geom_node(g0, g1, ls, step, i + 1, n) : xi;
+        const double c = 0.5 * ((xp - xi) + (xi - xm));
+        const double f = (xi >= C.gamma_min && xi <= C.gamma_max) ? pow(xi, -C.p) : 0.0;
+        const double w = c * f;
+        T.nt_w[i] = w;
+        T.nt_lg[i] = w != 0.0 ? 2.0 * log(xi) : 0.0;
     }
 }
 
