@@ -53,6 +53,13 @@ def test_sizes_without_gpu():
     assert lib.bhn_render_scratch_bytes(256) > lib.bhn_render_scratch_bytes(1)
     nb = lib.bhn_brick_tables_bytes(256, 128, 256)
     assert nb % 16 == 0 and nb >= 128 + 12 * (256 + 128 + 256)
+    from blackhole_native import grrt
+
+    g = grrt._declare()
+    one, four = g.bhn_grrt_scratch_bytes(14400, 1), g.bhn_grrt_scratch_bytes(14400, 4)
+    assert 0 < one < four and four - one >= 3 * 14400 * grrt.SEGMENT_BYTES
+    assert g.bhn_grrt_scratch_bytes(-1, 1) == -1 and g.bhn_grrt_scratch_bytes(10, 0) == -1
+    assert grrt.default_chunk(14400) == 198 and grrt.default_chunk(10**7) == 16 and grrt.default_chunk(1) == 256
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
