@@ -370,6 +370,20 @@ def bench_ours(args) -> dict | None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(brick_h, args.cpu_seconds)
 
+    # accuracy of the timed method (outside the timed region): a quarter-size
+    # crop from just outside the shadow through the torus image (3.75 M to
+    # 13.75 M right of centre) against the FP64 kernel at h/4, and the FP32
+    # Hamiltonian drift there
+    accuracy = None
+    if not args.no_accuracy:
+        from blackhole_native import studies
+
+        db64 = bn.DeviceBrick(brick_h, device=device, precisions=("fp32", "fp64"))
+        crop = (view.width // 2 + view.width * 3 // 32, view.height // 2 - view.height // 8, view.width // 4,
+                view.height // 4)
+        accuracy = studies.fine_step_check(db64, view, crop, config=cfg)
+        del db64
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -386,7 +400,9 @@ def bench_ours(args) -> dict | None:
         "e2e": e2e, "gpu_launches": K, "clocks": clk, "roofline": roofline, "roofline_fp32": roofline_fp32,
         "cpu_baseline": cpu,
         "kernel_ms": {"mean": statistics.mean(per_launch_ms), "min": min(per_launch_ms), "max": max(per_launch_ms)},
-        "status_counts": st2.status, "max_h_drift": st2.max_h_drift,
+        "status_counts": st2.status,
+        "h_drift": {"max_all_rays": st2.max_h_drift, "max_escaped_rays": st2.max_h_drift_escaped},
+        "accuracy": accuracy,
     }
     rnd.release_graph()
     if world > 1:
@@ -845,6 +861,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the crop check against the FP64 kernel at a quarter of the step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")

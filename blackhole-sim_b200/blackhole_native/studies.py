@@ -183,6 +183,43 @@ def precision_study(side: int = 4096, max_steps: int = 8192, log=print) -> dict:
     return out
 
 
+def fine_step_check(db: DeviceBrick, view: View, crop: tuple[int, int, int, int], fine: int = 4,
+                    config: RenderConfig | None = None) -> dict:
+    """Stokes error and Hamiltonian drift of the FP32 kernel on a crop of
+    ``view`` against the FP64 kernel at 1/``fine`` of the step (with ``fine``
+    times the step budget): errors over the pixels whose fine-step FP64 result
+    is stable under a 1e-6 step and camera-distance scaling and kept the null
+    constraint (|H - H0| <= MAX_DRIFT), plus FP32 against FP64 at the same
+    step on the pixels where the method at that step is itself stable.
+    ``db`` must hold both record precisions."""
+    v = replace(view, crop=crop)
+    vf = replace(v.scaled_step(1.0 / fine), max_steps=v.max_steps * fine)
+    ref_res = _render(db, vf, "fp64", ray_outputs=True)[0]
+    ref = ref_res.image().cpu().numpy()
+    ref_drift = ref_res.per_ray("h_drift").cpu().numpy().astype(np.float64)
+    del ref_res
+    perts = [_render(db, w, "fp64")[0].image().cpu().numpy() for w in (vf.scaled_step(1 + 1e-6), camera_perturbed(vf))]
+    scale = median_lit(ref[..., 0])
+    mask = stable_mask(ref, perts, scale) & (ref_drift <= MAX_DRIFT)
+    r32 = _render(db, v, "fp32", config=config, ray_outputs=True)[0]
+    img32 = r32.image().cpu().numpy()
+    drift32 = r32.per_ray("h_drift").cpu().numpy().astype(np.float64)
+    status32 = r32.per_ray("status").cpu().numpy()
+    r64 = _render(db, v, "fp64", ray_outputs=True)[0]
+    img64 = r64.image().cpu().numpy()
+    drift64 = r64.per_ray("h_drift").cpu().numpy().astype(np.float64)
+    p64 = [_render(db, w, "fp64")[0].image().cpu().numpy() for w in (v.scaled_step(1 + 1e-6), camera_perturbed(v))]
+    mask1 = stable_mask(img64, p64, median_lit(img64[..., 0])) & (drift64 <= MAX_DRIFT)
+    e_fine = image_errors(img32, ref, mask, scale)
+    e_same = image_errors(img32, img64, mask1, scale)
+    return {"crop": list(crop), "fine_step_factor": 1.0 / fine,
+            "mask_fraction": {"fine_step": float(mask.mean()), "same_step": float(mask1.mean())},
+            "fp32_vs_fp64_fine": {k: e_fine[k] for k in ("rel_l1_I", "rel_l1_Q", "rel_l1_U", "rel_l1_V",
+                                                         "flux_weighted_dm", "bad_frac")},
+            "fp32_vs_fp64_same_step": {k: e_same[k] for k in ("rel_l1_I", "flux_weighted_dm", "bad_frac")},
+            "h_drift_fp32": _drift_summary(drift32, status32)}
+
+
 def learned_study(net: learned.StepNet, side: int = 2048, log=print,
                   scenes_=((0.9375, 30.0), (0.998, 75.0))) -> dict:
     cfg = cached_config("image1024", torch.device("cuda"))

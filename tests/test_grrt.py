@@ -169,3 +169,37 @@ def test_gpu_chunk_does_not_change_the_image(golden, exact):
             img, d = (t.cpu().numpy() for t in grrt.render_stokes_image_device(cfg, snap, sc, diagnostics=True,
                                                                              chunk=chunk))
             assert np.array_equal(img, ref) and np.array_equal(d, ref_d), (max_tau, chunk)
+
+
+@pytest.mark.gpu
+def test_gpu_edge_cases(golden):
+    """No steps at all; a camera inside the snapshot whose rays run out of
+    steps while they emit (against the oracle); the renderer's argument checks."""
+    from blackhole_native import grrt
+
+    snap, sc = _snapshot(golden), _scaling(golden)
+    cam = golden["cam"]
+    cfg0 = grrt.PolarizedRenderConfig(width=5, height=4, camera=grrt.LocalCamera(*cam), step=0.1, max_steps=0)
+    img, d = (t.cpu().numpy() for t in grrt.render_stokes_image_device(cfg0, snap, sc, diagnostics=True))
+    assert not np.any(img) and np.all(d[..., 6] == 0) and np.all(d[..., 7] == 0)  # 0 steps, BHN_RAY_MAX_STEPS
+
+    inside = grrt.LocalCamera.from_degrees(r=12.0, inclination_degrees=80.0, fov_y_degrees=50.0)
+    cfg = grrt.PolarizedRenderConfig(width=6, height=4, camera=inside, step=0.1, max_steps=37)
+    img, d = (t.cpu().numpy() for t in grrt.render_stokes_image_device(cfg, snap, sc, diagnostics=True, chunk=5))
+    assert np.all(d[..., 6] <= 37) and np.any(d[..., 7] == 0) and np.any(d[..., 1] > 0)
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = float(golden["in_spin_a"]), inside.r, inside.theta, inside.phi
+    v.fov_y_deg, v.roll_deg, v.width, v.height = inside.fov_y_degrees, 0.0, 6, 4
+    scaling = dict(rho_cgs_per_code=float(golden["in_rho_cgs_per_code"]),
+                   b_gauss_per_code=float(golden["in_b_gauss_per_code"]))
+    for px, py in ((0, 0), (3, 2), (5, 3)):
+        S, (tau, e, va) = G.trace_pixel(v, _fields(golden), golden["in_r"], golden["in_theta"], golden["in_phi"],
+                                        scaling, 230e9, 0.1, 37, 220.0, length_cm=float(golden["in_rg_cm"]),
+                                        px=px, py=py)
+        assert e == d[py, px, 1] and va == d[py, px, 2]
+        assert _rel(img[py, px], S) <= 1e-10 if np.any(S) else not np.any(img[py, px])
+
+    with pytest.raises(ValueError, match="step must be finite and positive"):
+        grrt.render_stokes_image_device(grrt.PolarizedRenderConfig(width=2, height=2, step=0.0), snap, sc)
+    with pytest.raises(ValueError, match="chunk must be positive"):
+        grrt.render_stokes_image_device(cfg, snap, sc, chunk=0)
