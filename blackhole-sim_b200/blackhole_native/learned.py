@@ -22,7 +22,7 @@ Pipeline (all compute in this package's CUDA kernels):
    brick_scale times its step.
 
 The plain fixed-step RK2 method stays the reference: ``render_plain`` and the
-FP64 kernel at a finer step judge the learned method's image error.
+FP64 kernel at a finer step measure the learned method's image error.
 """
 
 from __future__ import annotations

@@ -119,3 +119,32 @@ def test_rejects_bad_models(golden):
             snap, scaling, coeff_model=syn.NonthermalPowerLawSynchrotronCoefficients(gamma_min=10.0, gamma_max=5.0))
     with pytest.raises(ValueError, match="dtype"):
         bn.precompute_coefficient_bricks(snap, scaling, dtype="float16")
+
+
+def test_extreme_plasma_regimes_against_oracle():
+    """Cells far from the fixtures' plasma: Theta_e from 1e-3 (nearly every
+    thermal Lorentz-factor node in the kernel table's far tail, where the GPU
+    skips it) to 1e3, |B| from 1e-3 to 1e3 code units, zero density; the
+    float64 brick against the oracle cell by cell."""
+    import itertools
+
+    rng = np.random.default_rng(9)
+    cells = []
+    for te, bs, rho in itertools.product((1e-3, 0.05, 1.0, 30.0, 1e3), (1e-3, 1.0, 1e3), (0.0, 1e-3, 1.0)):
+        for _ in range(2):
+            b = rng.normal(size=4)
+            b[1:] *= bs / np.linalg.norm(b[1:])
+            cells.append((rho, te, b))
+    n = len(cells)
+    rho = np.array([c[0] for c in cells]).reshape(n, 1, 1)
+    te = np.array([c[1] for c in cells]).reshape(n, 1, 1)
+    bc = np.array([c[2] for c in cells]).reshape(n, 1, 1, 4)
+    snap = SimpleNamespace(r=np.arange(n, dtype=np.float64) + 2.0, theta=np.array([1.0]), phi=np.array([0.0]), rho=rho,
+                           theta_e=te, b_con=bc, spin_a=0.9)
+    scaling = SimpleNamespace(rho_cgs_per_code=3e-18, b_gauss_per_code=25.0, mean_molecular_weight_per_electron=1.0)
+    got = bn.precompute_coefficient_bricks(snap, scaling, nu_hz=230e9, dtype="float64").coeffs
+    ref = S.precompute(rho, te, bc, 230e9, 3e-18, 25.0, dtype="float64")
+    assert np.array_equal(got == 0.0, ref == 0.0) and np.any(ref != 0.0)
+    assert _err(got, ref) <= 1e-12
+    nz = ref != 0.0
+    assert np.max(np.abs(got[nz] - ref[nz]) / np.abs(ref[nz])) <= 1e-10
