@@ -135,12 +135,13 @@ def test_extreme_plasma_regimes_against_oracle():
             b = rng.normal(size=4)
             b[1:] *= bs / np.linalg.norm(b[1:])
             cells.append((rho, te, b))
-    n = len(cells)
-    rho = np.array([c[0] for c in cells]).reshape(n, 1, 1)
-    te = np.array([c[1] for c in cells]).reshape(n, 1, 1)
-    bc = np.array([c[2] for c in cells]).reshape(n, 1, 1, 4)
-    snap = SimpleNamespace(r=np.arange(n, dtype=np.float64) + 2.0, theta=np.array([1.0]), phi=np.array([0.0]), rho=rho,
-                           theta_e=te, b_con=bc, spin_a=0.9)
+    cells += cells[: -len(cells) % 4]  # a [n][2][2] brick (grids need two values per axis)
+    n = len(cells) // 4
+    rho = np.array([c[0] for c in cells]).reshape(n, 2, 2)
+    te = np.array([c[1] for c in cells]).reshape(n, 2, 2)
+    bc = np.array([c[2] for c in cells]).reshape(n, 2, 2, 4)
+    snap = SimpleNamespace(r=np.arange(n, dtype=np.float64) + 2.0, theta=np.array([1.0, 2.0]), phi=np.array([0.0, 3.0]),
+                           rho=rho, theta_e=te, b_con=bc, spin_a=0.9)
     scaling = SimpleNamespace(rho_cgs_per_code=3e-18, b_gauss_per_code=25.0, mean_molecular_weight_per_electron=1.0)
     got = bn.precompute_coefficient_bricks(snap, scaling, nu_hz=230e9, dtype="float64").coeffs
     ref = S.precompute(rho, te, bc, 230e9, 3e-18, 25.0, dtype="float64")
