@@ -168,12 +168,94 @@ def precompute_device_coefficients(snapshot, scaling, nu_hz: float = 230e9,
     return r, theta, phi, out
 
 
+PIPELINE_MIN_CELLS = 1 << 20   # host-to-host calls this large are pipelined in r slabs
+PIPELINE_SLABS = 8
+
+
 def precompute_coefficient_bricks(snapshot, scaling, nu_hz: float = 230e9,
                                   dtype: Literal["float32", "float64"] = "float32", coeff_model=None,
                                   stride: int = 1) -> BrickGrid:
-    """coefficient_bricks.py:119-152 on the GPU; returns the host brick."""
-    r, theta, phi, out = precompute_device_coefficients(snapshot, scaling, nu_hz, dtype, coeff_model, stride)
-    return BrickGrid(r, theta, phi, out.cpu().numpy(), spin_a=float(snapshot.spin_a))
+    """coefficient_bricks.py:119-152 on the GPU; returns the host brick.
+
+    Large snapshots go through in r slabs: while the device computes slab k,
+    slab k + 1's fields are staged in pinned memory and uploaded on a copy
+    stream and slab k - 1's coefficients come back on another, so the
+    transfers hide behind the kernel.  Slabs change no value."""
+    if dtype not in ("float32", "float64"):
+        raise ValueError("dtype must be 'float32' or 'float64'")
+    r, theta, phi, rho, theta_e, b_con = _fields(snapshot, stride)
+    shape = (r.size, theta.size, phi.size)
+    if int(np.prod(shape)) < PIPELINE_MIN_CELLS or r.size < 2 * PIPELINE_SLABS:
+        r, theta, phi, out = precompute_device_coefficients(snapshot, scaling, nu_hz, dtype, coeff_model, stride)
+        return BrickGrid(r, theta, phi, out.cpu().numpy(), spin_a=float(snapshot.spin_a))
+    coeffs = _precompute_pipelined(rho, theta_e, b_con, scaling, nu_hz, dtype, coeff_model)
+    return BrickGrid(r, theta, phi, coeffs, spin_a=float(snapshot.spin_a))
+
+
+def _precompute_pipelined(rho: np.ndarray, theta_e: np.ndarray, b_con: np.ndarray, scaling, nu_hz: float,
+                          dtype: str, coeff_model) -> np.ndarray:
+    L = _declare()
+    device = dev.require_cuda()
+    nr = rho.shape[0]
+    plane = int(np.prod(rho.shape[1:]))
+    slab = -(-nr // PIPELINE_SLABS)
+    cap = slab * plane
+    ndt = np.float32 if dtype == "float32" else np.float64
+    tdt = torch.float32 if dtype == "float32" else torch.float64
+    out_host = np.empty(rho.shape + (11,), dtype=ndt)
+    m = model_struct(coeff_model or HybridSynchrotronCoefficients(), nu_hz, scaling)
+    f64 = dict(dtype=torch.float64)
+    h_in = [[torch.empty(cap, **f64).pin_memory(), torch.empty(cap, **f64).pin_memory(),
+             torch.empty(cap * 4, **f64).pin_memory()] for _ in range(2)]
+    d_in = [[torch.empty(cap, device=device, **f64), torch.empty(cap, device=device, **f64),
+             torch.empty(cap * 4, device=device, **f64)] for _ in range(2)]
+    h_out = [torch.empty(cap * 11, dtype=tdt).pin_memory() for _ in range(2)]
+    d_out = [torch.empty(cap * 11, dtype=tdt, device=device) for _ in range(2)]
+    compute = torch.cuda.current_stream(device)
+    up, down = torch.cuda.Stream(device), torch.cuda.Stream(device)
+    up.wait_stream(compute)
+    down.wait_stream(compute)
+    uploaded = [torch.cuda.Event() for _ in range(2)]
+    computed = [torch.cuda.Event() for _ in range(2)]
+    downloaded = [torch.cuda.Event() for _ in range(2)]
+    rflat, tflat, bflat = rho.reshape(nr, -1), theta_e.reshape(nr, -1), b_con.reshape(nr, -1)
+    slabs = [(k * slab, min(nr, (k + 1) * slab)) for k in range(PIPELINE_SLABS) if k * slab < nr]
+
+    def finish(k):  # slab k's coefficients are on the host: copy them out of the pinned buffer
+        a, b = slabs[k]
+        downloaded[k % 2].synchronize()
+        out_host[a:b] = h_out[k % 2][: (b - a) * plane * 11].numpy().reshape((b - a,) + rho.shape[1:] + (11,))
+
+    for k, (a, b) in enumerate(slabs):
+        j, n = k % 2, (b - a) * plane
+        if k >= 2:
+            uploaded[j].synchronize()  # slab k - 2's upload has left this pinned buffer
+        h_in[j][0][:n].numpy()[:] = rflat[a:b].reshape(-1)
+        h_in[j][1][:n].numpy()[:] = tflat[a:b].reshape(-1)
+        h_in[j][2][: 4 * n].numpy()[:] = bflat[a:b].reshape(-1)
+        with torch.cuda.stream(up):
+            if k >= 2:
+                up.wait_event(computed[j])  # slab k - 2's kernel has read these device inputs
+            for dst, src, cnt in zip(d_in[j], h_in[j], (n, n, 4 * n)):
+                dst[:cnt].copy_(src[:cnt], non_blocking=True)
+            uploaded[j].record(up)
+        compute.wait_event(uploaded[j])
+        if k >= 2:
+            compute.wait_event(downloaded[j])  # slab k - 2's coefficients have left this device buffer
+        _lib.check(L.bhn_brick_precompute(dev.ptr(d_in[j][0]), dev.ptr(d_in[j][1]), dev.ptr(d_in[j][2]), n,
+                                          ctypes.byref(m), dev.ptr(d_out[j]), 4 if dtype == "float32" else 8,
+                                          compute.cuda_stream))
+        computed[j].record(compute)
+        if k >= 1:
+            finish(k - 1)  # while slab k computes; frees h_out[(k - 1) % 2] for slab k + 1
+        with torch.cuda.stream(down):
+            down.wait_event(computed[j])
+            h_out[j][: 11 * n].copy_(d_out[j][: 11 * n], non_blocking=True)
+            downloaded[j].record(down)
+    finish(len(slabs) - 1)
+    compute.wait_stream(up)
+    compute.wait_stream(down)
+    return out_host
 
 
 def precompute_device_brick(snapshot, scaling, nu_hz: float = 230e9, coeff_model=None, stride: int = 1,

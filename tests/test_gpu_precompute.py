@@ -149,3 +149,18 @@ def test_extreme_plasma_regimes_against_oracle():
     assert _err(got, ref) <= 1e-12
     nz = ref != 0.0
     assert np.max(np.abs(got[nz] - ref[nz]) / np.abs(ref[nz])) <= 1e-10
+
+
+def test_pipelined_host_path_equals_device_path():
+    """A snapshot above the pipelining threshold: the host-to-host call (r
+    slabs through pinned buffers on copy streams) returns exactly the
+    device-resident result, for both output precisions."""
+    from blackhole_native import grrt
+
+    snap = grrt.seeded_snapshot(20, 256, 256, seed=3)   # 1.3M cells, 20 r shells
+    scaling = SimpleNamespace(rho_cgs_per_code=3e-18, b_gauss_per_code=25.0, mean_molecular_weight_per_electron=1.0)
+    assert snap.rho.size >= syn.PIPELINE_MIN_CELLS
+    for dtype in ("float32", "float64"):
+        host = bn.precompute_coefficient_bricks(snap, scaling, dtype=dtype)
+        dev_out = syn.precompute_device_coefficients(snap, scaling, dtype=dtype)[3].cpu().numpy()
+        assert host.coeffs.dtype == dev_out.dtype and np.array_equal(host.coeffs, dev_out)
