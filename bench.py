@@ -375,7 +375,7 @@ def bench_ours(args) -> dict | None:
     # 13.75 M right of centre) against the FP64 kernel at h/4, and the FP32
     # Hamiltonian drift there
     accuracy = None
-    if not args.no_accuracy:
+    if rank == 0 and not args.no_accuracy:
         from blackhole_native import studies
 
         db64 = bn.DeviceBrick(brick_h, device=device, precisions=("fp32", "fp64"))
