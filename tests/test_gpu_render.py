@@ -325,3 +325,19 @@ def test_view_sweep_against_oracle(name):
     g32 = bn.render(db, vg, precision="fp32").image().cpu().numpy().astype(np.float64)
     assert rel_l1(g32[ok][:, 0], g_img[ok][:, 0]) <= FP32_I_REL_L1
     assert flux_weighted_dm(g32[ok], g_img[ok]) <= FP32_DM
+
+
+def test_fine_step_check_reports_the_method_error(scene_brick):
+    """The bench's accuracy block (studies.fine_step_check) on a small crop of
+    the bench scene: most pixels pass the stability mask, the FP32 kernel sits
+    within the FP32 bar of the FP64 kernel at the same step and within the
+    method's own step error of the FP64 kernel at a quarter of it."""
+    from blackhole_native import studies
+
+    b, db = scene_brick
+    v = bn.View(256, 256, max_steps=4096)
+    acc = studies.fine_step_check(db, v, (152, 96, 32, 64))
+    assert acc["mask_fraction"]["fine_step"] > 0.9 and acc["mask_fraction"]["same_step"] > 0.9
+    assert acc["fp32_vs_fp64_same_step"]["rel_l1_I"] <= 1e-4
+    assert 0.0 < acc["fp32_vs_fp64_fine"]["rel_l1_I"] <= 1e-2
+    assert acc["h_drift_fp32"]["median_escaped"] <= 1e-3
