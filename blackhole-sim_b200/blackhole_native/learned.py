@@ -30,7 +30,7 @@ from __future__ import annotations
 import ctypes
 import json
 import math
-from dataclasses import dataclass, replace
+from dataclasses import dataclass
 from pathlib import Path
 from typing import Sequence
 

@@ -9,7 +9,6 @@
 
 from __future__ import annotations
 
-import math
 from dataclasses import replace
 
 import numpy as np
