@@ -268,3 +268,39 @@ def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diag
 def render_stokes_image(cfg, snapshot, scaling, progress: bool = False, *, coeff_model=None):
     """polarized_renderer.py:56-70 on the GPU: the (H, W, 4) float64 Stokes image."""
     return render_stokes_image_device(cfg, snapshot, scaling, coeff_model=coeff_model).cpu().numpy()
+
+
+def _host_image(stokes_img) -> np.ndarray:
+    if isinstance(stokes_img, torch.Tensor):
+        stokes_img = stokes_img.detach().cpu().numpy()
+    return np.asarray(stokes_img, dtype=np.float64)
+
+
+def stokes_to_rgb(stokes_img, gamma: float = 2.2) -> np.ndarray:
+    """polarized_renderer.py:80-95: the diagnostic colour image of an (H, W, 4)
+    Stokes image, (H, W, 3) float64 in [0, 1].  Brightness follows I (negative
+    I clipped to 0); the linear polarization sqrt(Q^2 + U^2) adds green, the
+    signs of Q and V tint red / blue; every channel is divided by the 99.5th
+    percentile of all three, compressed as x / (1 + x) and gamma-encoded.
+    Host post-processing of a rendered image (device tensors are copied back)."""
+    s = _host_image(stokes_img)
+    i = np.maximum(s[..., 0], 0.0)
+    q, u, v = s[..., 1], s[..., 2], s[..., 3]
+    lin = np.sqrt(q * q + u * u)
+    rgb = np.stack([i + 0.35 * np.maximum(q, 0.0) + 0.15 * np.maximum(v, 0.0),
+                    i + 0.25 * lin,
+                    i + 0.35 * np.maximum(-q, 0.0) + 0.15 * np.maximum(-v, 0.0)], axis=-1)
+    peak = float(np.percentile(rgb, 99.5)) if np.any(rgb > 0.0) else 1.0
+    rgb = rgb / max(peak, 1.0e-300)
+    rgb = rgb / (1.0 + rgb)
+    return np.clip(rgb, 0.0, 1.0) ** (1.0 / gamma)
+
+
+def save_stokes_npz(stokes_img, path) -> None:
+    """polarized_renderer.py:98-101: the image as float64 under the key
+    ``stokes`` in a compressed npz, parent directories created."""
+    from pathlib import Path
+
+    p = Path(path)
+    p.parent.mkdir(parents=True, exist_ok=True)
+    np.savez_compressed(p, stokes=_host_image(stokes_img))

@@ -409,10 +409,22 @@ def brick_npz_fixture(cb, path) -> None:
     cb.CoefficientBrickGrid(r, theta, phi, coeffs, 86e9, 0.5, "float32").save_npz(path)
 
 
+def rgb_fixtures(pr) -> dict[str, np.ndarray]:
+    """polarized_renderer.stokes_to_rgb (polarized_renderer.py:80-95) on a seeded
+    Stokes image with negative I, Q and V entries and an all-dark image."""
+    rng = np.random.default_rng(12)
+    img = rng.normal(0.0, 1.0, (16, 24, 4)) * np.array([1.0, 0.3, 0.3, 0.1])
+    img[..., 0] = np.abs(img[..., 0]) * 1e-3
+    img[3, 5, 0] = -0.5
+    dark = np.zeros((4, 6, 4))
+    return {"rgb_in": img, "rgb_out": pr.stokes_to_rgb(img), "rgb_out_g18": pr.stokes_to_rgb(img, gamma=1.8),
+            "rgb_dark_in": dark, "rgb_dark_out": pr.stokes_to_rgb(dark)}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/python")
-    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz")
+    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
@@ -445,6 +457,9 @@ def main() -> None:
     if not only or "grrt" in only:
         np.savez_compressed(HERE / "grrt.npz", **grrt_fixtures(grmhd, calibration, kerr, pr))
         print("wrote grrt.npz")
+    if not only or "rgb" in only:
+        np.savez_compressed(HERE / "stokes_rgb.npz", **rgb_fixtures(pr))
+        print("wrote stokes_rgb.npz")
 
 
 if __name__ == "__main__":

@@ -203,3 +203,20 @@ def test_gpu_edge_cases(golden):
         grrt.render_stokes_image_device(grrt.PolarizedRenderConfig(width=2, height=2, step=0.0), snap, sc)
     with pytest.raises(ValueError, match="chunk must be positive"):
         grrt.render_stokes_image_device(cfg, snap, sc, chunk=0)
+
+
+def test_stokes_to_rgb_and_npz_match_the_reference(tmp_path):
+    """polarized_renderer.stokes_to_rgb / save_stokes_npz against the
+    reference's own outputs (tests/golden/stokes_rgb.npz)."""
+    from blackhole_native import grrt
+
+    with np.load(Path(__file__).parent / "golden" / "stokes_rgb.npz") as z:
+        g = {k: z[k] for k in z}
+    assert np.array_equal(grrt.stokes_to_rgb(g["rgb_in"]), g["rgb_out"])
+    assert np.array_equal(grrt.stokes_to_rgb(g["rgb_in"], gamma=1.8), g["rgb_out_g18"])
+    assert np.array_equal(grrt.stokes_to_rgb(g["rgb_dark_in"]), g["rgb_dark_out"])
+    out = tmp_path / "a" / "b" / "img.npz"
+    grrt.save_stokes_npz(g["rgb_in"].astype(np.float32), out)
+    with np.load(out) as z:
+        assert list(z.keys()) == ["stokes"] and z["stokes"].dtype == np.float64
+        assert np.array_equal(z["stokes"], g["rgb_in"].astype(np.float32).astype(np.float64))
