@@ -99,9 +99,13 @@ def sum_over_ranks(value: float, world: int, device) -> float:
 
 def barrier(world: int) -> None:
     if world > 1:
+        import torch
         import torch.distributed as td
 
-        td.barrier()
+        if td.get_backend() == "nccl":  # name this rank's GPU: NCCL would otherwise guess one
+            td.barrier(device_ids=[torch.cuda.current_device()])
+        else:
+            td.barrier()
 
 
 class ClockSampler:
