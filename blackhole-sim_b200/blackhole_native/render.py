@@ -402,7 +402,8 @@ class PipelinedRenderer:
     """Renders a sequence of bricks on the same grids (successive snapshots of
     a simulation, say) for fixed views, overlapping data movement with the
     kernel: while brick k renders, brick k + 1 is copied from pinned host memory
-    on a copy stream and image k - 1 is copied back on a third stream.  Two
+    and packed into records on a copy stream and image k - 1 is copied back on
+    a third stream.  Two
     record buffers, two raw staging buffers and two compiled launches
     alternate; events order every buffer's reuse.  Host bricks must be pinned
     (``tensor.pin_memory()``) for the copies to overlap."""
@@ -441,13 +442,15 @@ class PipelinedRenderer:
             if self.staging[s] is None or self.staging[s].dtype != src.dtype:
                 self.staging[s] = torch.empty(cells, dtype=src.dtype, device=self.bricks[0].device)
             with torch.cuda.stream(self.copy_stream):
-                if k >= 2:  # staging[s] is free once brick k - 2 has been packed
-                    self.copy_stream.wait_event(self.packed[s])
+                # staging[s] and the records of bricks[s] are packed / rendered in
+                # stream order here; the records are free once image k - 2 has rendered
                 self.staging[s].copy_(src, non_blocking=True)
                 self.copied[s].record(self.copy_stream)
-            compute.wait_event(self.copied[s])
-            self.bricks[s]._pack(self.staging[s], self.precision, check_finite=False)
-            self.packed[s].record(compute)
+                if k >= 2:
+                    self.copy_stream.wait_event(self.rendered[s])
+                self.bricks[s]._pack(self.staging[s], self.precision, check_finite=False)  # beside render k - 1
+                self.packed[s].record(self.copy_stream)
+            compute.wait_event(self.packed[s])
             if k >= 2:  # the output buffer is free once image k - 2 has been fetched
                 compute.wait_event(self.fetched[s])
             self.renderers[s].graph_launch()
