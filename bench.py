@@ -15,8 +15,10 @@ oracle, OpenMP over every host core) on a bounded sample of the same workload.
 
 Other workloads (--workload): views (256 uneven views in one launch),
 precompute (coefficient bricks from a 256 x 128 x 256 seeded snapshot, cells/s)
-and grrt (the physical polarized renderer's default 160 x 90 image, pixels/s);
-their lines carry an FP64 exp() roofline measured in the same run.
+and grrt (the physical polarized renderer's default 160 x 90 image, pixels/s),
+whose lines carry an FP64 exp() roofline measured in the same run; learned
+(time to an image at 1e-3 Stokes-I error: the learned step size against plain
+RK2 and the step-doubling controller).
 For N > 1 the job runs as torchrun ranks, one full image per rank (replicas:
 rays are independent and the path has no exchange step).
 """
@@ -825,6 +827,70 @@ def _lib_check(rc):
     _lib.check(rc)
 
 
+# ------------------------------------------------------------------ learned step size
+def bench_learned(args) -> dict | None:
+    """Time to an image at <= 1e-3 Stokes-I rel L1 against the FP64 kernel at
+    h/16: plain fixed-step RK2 at h, h/2, h/4, h/8 against the learned step
+    size and the step-doubling controller, on a 2048x2048 view (a = 0.9375,
+    i = 30 deg, horizon guard on) of a seeded torus brick (seed 1).  The
+    error is taken over pixels whose fine-step result is stable and kept the
+    null constraint (studies.py)."""
+    import torch
+
+    from blackhole_native import learned, studies
+    from blackhole_native.bricks import torus_brick
+    from blackhole_native.render import DeviceBrick, View
+
+    rank, world, local_rank = dist_env()
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local_rank)
+    side = args.side or 2048
+    spin, incl = 0.9375, 30.0
+    db = DeviceBrick(torus_brick(256, 128, 256, spin_a=spin, seed=1), precisions=("fp32", "fp64"))
+    v = View(side, side, spin_a=spin, inclination_deg=incl, max_steps=65536, horizon_guard=True)
+    v16 = v.scaled_step(1 / 16)
+    ref_res = studies._render(db, v16, "fp64", ray_outputs=True)[0]
+    ref = ref_res.image().cpu().numpy()
+    drift = ref_res.per_ray("h_drift").cpu().numpy().astype(np.float64)
+    del ref_res
+    ref8 = studies._render(db, v.scaled_step(1 / 8), "fp64")[0].image().cpu().numpy()
+    perts = [studies._render(db, w, "fp64")[0].image().cpu().numpy()
+             for w in (v.scaled_step(1 / 16 * (1 + 1e-6)), studies.camera_perturbed(v16))]
+    scale = studies.median_lit(ref[..., 0])
+    mask = studies.stable_mask(ref, perts, scale) & np.isfinite(ref8[..., 0]) & (
+        np.abs(ref8[..., 0] - ref[..., 0]) <= 1e-2 * np.abs(ref[..., 0]) + 1e-4 * scale) & (drift <= studies.MAX_DRIFT)
+    net = learned.shipped_weights()
+    if net is None:
+        raise RuntimeError("the shipped step-size network (weights/step_net.npz) is missing")
+    reps = max(args.steps, 1)
+    runs = {}
+    for f in (1.0, 0.5, 0.25, 0.125):
+        runs[f"plain h*{f}"] = learned.render_plain(db, [v.scaled_step(f)], repeats=reps)
+    runs["learned"] = learned.render_learned(db, [v], net, learned.AdaptConfig(), repeats=reps)
+    runs["controller tol 1e-5"] = learned.render_adaptive(db, [v], learned.AdaptConfig(tol=1e-5), repeats=reps)
+    table = {}
+    for k, r in runs.items():
+        e = studies.image_errors(r.image().cpu().numpy(), ref, mask, scale)
+        table[k] = {"ms": round(r.ms, 2), "rel_l1_I": e["rel_l1_I"], "capped_rel_l1_I": e["capped_rel_l1_I"],
+                    "bad_frac": e["bad_frac"], **({"rhs_evals": r.counters["rhs_evals"]} if r.counters else {})}
+    ok = {k: t["ms"] for k, t in table.items() if t["rel_l1_I"] <= 1e-3}
+    plain_best = min((t for k, t in ok.items() if k.startswith("plain")), default=None)
+    learned_ms = ok.get("learned")
+    return {
+        "metric": "time to an image at <= 1e-3 Stokes-I rel L1 vs the FP64 fine-step kernel (learned step size)",
+        "value": learned_ms, "unit": "ms", "n_gpus": 1, "steps": reps, "warmup": None, "ms_per_step": learned_ms,
+        "timing": "each method: the fastest of `steps` launches (CUDA events)",
+        "higher_is_better": False, "scaling": "none", "vs_baseline": None, "dtype": "f32 (BF16 network)",
+        "data": "synthetic",
+        "config": {"workload": f"learned step size: {side}x{side} rays, a={spin}, i={incl}deg, horizon guard, "
+                               "256x128x256x11 float32 torus brick (seed 1), reference FP64 kernel at h/16",
+                   "mask_fraction": float(mask.mean())},
+        "plain_best_ms": plain_best, "speedup_vs_plain": (plain_best / learned_ms) if plain_best and learned_ms else None,
+        "runs": table, "gpu_launches": len(runs) * reps,
+    }
+
+
 def bench_reference(args) -> dict | None:
     rank, world, _ = dist_env()
     if rank != 0:
@@ -871,9 +937,10 @@ def main(argv=None) -> int:
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")
     ap.add_argument("--tune", action="store_true", help="run the launch-shape autotuner on the workload and exit")
-    ap.add_argument("--workload", choices=["image", "views", "precompute", "grrt"], default="image",
+    ap.add_argument("--workload", choices=["image", "views", "precompute", "grrt", "learned"], default="image",
                     help="image: the 1024x1024 single view (default); views: many uneven views in one launch; "
-                         "precompute: coefficient bricks from a snapshot; grrt: the physical polarized renderer")
+                         "precompute: coefficient bricks from a snapshot; grrt: the physical polarized renderer; "
+                         "learned: time to an image at 1e-3, learned step size against plain RK2")
     ap.add_argument("--n-views", type=int, default=256)
     ap.add_argument("--side", type=int, default=0,
                     help="profiling only: image workload side x side rays; precompute nr = side; grrt image "
@@ -888,6 +955,8 @@ def main(argv=None) -> int:
         line = bench_precompute(args)
     elif args.workload == "grrt":
         line = bench_grrt(args)
+    elif args.workload == "learned":
+        line = bench_learned(args)
     else:
         line = bench_ours(args)
     if line is not None:
