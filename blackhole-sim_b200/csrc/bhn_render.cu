@@ -1164,6 +1164,9 @@ int bhn_render_prepare(const bhn_view *h_views, int32_t n_views, void *scratch, 
         if (!(v.h_min > 0.0 && v.h_max >= v.h_min && std::isfinite(v.h_max) && std::isfinite(v.h_scale)))
             return fail(BHN_ERR_VALUE, "step bounds must satisfy 0 < h_min <= h_max");
         if (v.out_offset < 0) return fail(BHN_ERR_VALUE, "out_offset must be non-negative");
+        // the kernels keep a ray's output index in 32 bits
+        if (v.out_offset + (int64_t)v.crop_w * v.crop_h > ((int64_t)1 << 32))
+            return fail(BHN_ERR_VALUE, "views address more than 2^32 output pixels");
     }
     cudaStream_t s = as_stream(stream);
     char *sc = static_cast<char *>(scratch);

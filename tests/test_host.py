@@ -101,3 +101,21 @@ def test_brick_npz_round_trip(tmp_path):
     a.save_npz(tmp_path / "b.npz")
     b = bn.BrickGrid.load_npz(tmp_path / "b.npz")
     assert np.array_equal(a.coeffs, b.coeffs) and np.array_equal(a.r, b.r) and b.spin_a == 0.5
+
+
+def test_render_prepare_rejects_outputs_beyond_32_bit_indices():
+    """The kernels keep a ray's output index in 32 bits: bhn_render_prepare
+    refuses views whose packed outputs reach past 2^32 pixels (checked on the
+    host, before any device work)."""
+    import ctypes
+
+    from blackhole_native import _lib
+
+    L = _lib.lib()
+    L.bhn_render_prepare.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+    L.bhn_render_prepare.restype = ctypes.c_int
+    v = bn.View(1024, 1024).to_struct((1 << 32) - 1024 * 1024 + 1)
+    scratch = ctypes.create_string_buffer((1 << 16) + 256)
+    aligned = (ctypes.addressof(scratch) + 255) & ~255
+    rc = L.bhn_render_prepare(ctypes.byref(v), 1, aligned, 1 << 16, None)
+    assert rc == 1 and b"2^32" in L.bhn_last_error()
