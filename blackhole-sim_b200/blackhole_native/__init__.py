@@ -24,7 +24,7 @@ from .kernels import (sample_and_step_stokes, sample_brick_trilinear, sample_bri
                       stokes_rk2_brick)
 from .render import (DeviceBrick, PipelinedRenderer, RenderConfig, Renderer, RenderResult, RenderStats, View, render,
                      render_stokes)
-from . import grrt, tiles
+from . import accelerated, grrt, tiles
 from .synchrotron import (HybridSynchrotronCoefficients, NonthermalPowerLawSynchrotronCoefficients,
                           ThermalSynchrotronCoefficients, precompute_coefficient_bricks, precompute_device_brick)
 
@@ -35,7 +35,7 @@ __all__ = [
     "sample_brick_valid_mask", "COEFF_NAMES", "BrickGrid", "torus_brick", "horizon_radius", "DeviceBrick",
     "RenderConfig", "Renderer", "RenderResult", "RenderStats", "View", "render", "render_stokes", "PipelinedRenderer",
     "precompute_coefficient_bricks", "precompute_device_brick", "HybridSynchrotronCoefficients",
-    "ThermalSynchrotronCoefficients", "NonthermalPowerLawSynchrotronCoefficients", "grrt", "tiles",
+    "ThermalSynchrotronCoefficients", "NonthermalPowerLawSynchrotronCoefficients", "accelerated", "grrt", "tiles",
 ]
 
 

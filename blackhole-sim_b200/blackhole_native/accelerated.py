@@ -1,0 +1,139 @@
+"""The reference's own brick renderer on the GPU.
+
+Drop-in for ``render_stokes_image_bricks`` and ``render_tile_stokes_bricks``
+(python/blackhole_sim/accelerated_renderer.py:100-158): per pixel the camera
+ray, a fixed-step RK4 Kerr geodesic (kerr.py:306-313, 337-384) and
+``integrate_stokes_from_bricks_trace`` -- the coefficient brick sampled at each
+segment's midpoint, RK2 or exact Stokes steps, the optical-depth cutoff --
+in FP64, one thread per ray (``bhn_brick_trace_render``).  This is the
+reference Python's method; ``render`` / ``Renderer`` run the RK2 form with
+the step h = 0.02 r in FP32.
+
+The brick follows ``CoefficientBrickGrid`` (coefficient_bricks.py:28-49): its
+grids are float32 values, which set the sampled r / theta range.  The
+reference interpolates in the brick's dtype with float32 weights (NumPy's
+promotion of float32 grids); the GPU does it in float64, so images agree to
+float32 rounding.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _device as dev
+from . import _lib
+from .grrt import LocalCamera, PolarizedTransferConfig
+
+
+@dataclass(frozen=True)
+class AcceleratedRenderConfig:
+    """accelerated_renderer.py:36-46."""
+
+    width: int = 160
+    height: int = 90
+    camera: LocalCamera = field(default_factory=lambda: LocalCamera.from_degrees(r=55.0, inclination_degrees=65.0,
+                                                                                  fov_y_degrees=32.0))
+    step: float = 0.06
+    max_steps: int = 5000
+    escape_radius: float = 220.0
+    transfer: PolarizedTransferConfig = field(default_factory=lambda: PolarizedTransferConfig(use_exact_matrix_step=False))
+    tile_size: int = 64
+    progressive_min_width: int = 480
+
+
+class BrickTraceConfigStruct(ctypes.Structure):
+    """``bhn_brick_trace_config``."""
+
+    _fields_ = [
+        ("step", ctypes.c_double),
+        ("escape_radius", ctypes.c_double),
+        ("length_cm", ctypes.c_double),
+        ("max_optical_depth", ctypes.c_double),
+        ("max_steps", ctypes.c_int32),
+        ("exact_step", ctypes.c_int32),
+    ]
+
+
+DIAGNOSTICS = ("optical_depth", "sampled_segments", "steps", "status")
+
+
+def _declare() -> ctypes.CDLL:
+    L = _lib.lib()
+    fn = L.bhn_brick_trace_render
+    vp, i32 = ctypes.c_void_p, ctypes.c_int32
+    fn.argtypes = [vp, vp, i32, vp, i32, vp, i32, ctypes.POINTER(_lib.ViewStruct), ctypes.POINTER(BrickTraceConfigStruct),
+                   vp, ctypes.c_int64, vp, vp, vp]
+    fn.restype = ctypes.c_int
+    return L
+
+
+def _grid(g) -> np.ndarray:
+    """A brick axis as CoefficientBrickGrid stores it (float32 values), in float64."""
+    a = np.asarray(g, dtype=np.float32).astype(np.float64)
+    if a.ndim != 1 or a.size < 2 or np.any(np.diff(a) <= 0.0):
+        raise ValueError("brick grids must be strictly increasing 1-D arrays of at least 2 values")
+    return np.ascontiguousarray(a)
+
+
+def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagnostics: bool = False,
+                                      device: torch.device | None = None):
+    """(h, w, 4) float64 Stokes image of the tile (default: the whole image)
+    on the device, and (h, w, 4) diagnostics (columns ``DIAGNOSTICS``) when
+    asked.  ``snapshot`` supplies the spin (``spin_a``)."""
+    L = _declare()
+    device = device or dev.require_cuda()
+    coeffs = np.asarray(bricks.coeffs)
+    shape = tuple(np.asarray(getattr(bricks, n)).size for n in ("r", "theta", "phi"))
+    if coeffs.shape != shape + (11,):
+        raise ValueError(f"coeffs must have shape {shape + (11,)}; got {coeffs.shape}")
+    if not np.all(np.isfinite(coeffs)):
+        raise ValueError("coefficient brick contains non-finite values")
+    grids = [torch.as_tensor(_grid(getattr(bricks, n)), device=device) for n in ("r", "theta", "phi")]
+    d_coeffs = torch.as_tensor(np.ascontiguousarray(coeffs, dtype=np.float64), device=device)
+    cam = cfg.camera
+    W, H = int(cfg.width), int(cfg.height)
+    if W < 1 or H < 1:
+        raise ValueError("image width and height must be positive")
+    x0, y0, w, h = (0, 0, W, H) if tile is None else (int(tile.x0), int(tile.y0), int(tile.x1 - tile.x0),
+                                                       int(tile.y1 - tile.y0))
+    v = _lib.ViewStruct()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = float(snapshot.spin_a), float(cam.r), float(cam.theta), float(cam.phi)
+    v.fov_y_deg, v.roll_deg = float(cam.fov_y_degrees), float(getattr(cam, "roll_degrees", 0.0))
+    v.h_scale, v.h_min, v.h_max = 0.02, 1e-3, 1.0  # unused by the fixed-step loop
+    v.escape_radius, v.affine_to_length_cm, v.max_optical_depth = float(cfg.escape_radius), 1.0, 30.0
+    v.width, v.height, v.x0, v.y0, v.crop_w, v.crop_h = W, H, x0, y0, w, h
+    v.max_steps, v.flags, v.out_offset = int(cfg.max_steps), 0, 0
+    t = cfg.transfer
+    c = BrickTraceConfigStruct()
+    c.step, c.escape_radius = float(cfg.step), float(cfg.escape_radius)
+    c.length_cm = float(getattr(t, "affine_to_length_cm", None) or 1.0)  # accelerated_renderer.py:146
+    c.max_optical_depth, c.max_steps = float(t.max_optical_depth), int(cfg.max_steps)
+    c.exact_step = int(bool(t.use_exact_matrix_step))
+    nbytes = int(L.bhn_render_scratch_bytes(1))
+    scratch = torch.empty(nbytes // 8 + 64, dtype=torch.float64, device=device)
+    sp = (dev.ptr(scratch) + 255) & ~255
+    out = torch.empty((h, w, 4), dtype=torch.float64, device=device)
+    diag = torch.empty((h, w, 4), dtype=torch.float64, device=device) if diagnostics else None
+    _lib.check(L.bhn_brick_trace_render(dev.ptr(d_coeffs), dev.ptr(grids[0]), shape[0], dev.ptr(grids[1]), shape[1],
+                                        dev.ptr(grids[2]), shape[2], ctypes.byref(v), ctypes.byref(c), sp, nbytes,
+                                        dev.ptr(out), dev.ptr(diag), dev.stream_ptr()))
+    return (out, diag) if diagnostics else out
+
+
+def render_tile_stokes_bricks(cfg, snapshot, bricks, tile) -> np.ndarray:
+    """accelerated_renderer.py:129-150 on the GPU: the (tile.height, tile.width, 4) float64 block."""
+    return render_stokes_image_bricks_device(cfg, snapshot, bricks, tile=tile).cpu().numpy()
+
+
+def render_stokes_image_bricks(cfg, snapshot, bricks) -> np.ndarray:
+    """accelerated_renderer.py:153-158 on the GPU: the (H, W, 4) float64 image
+    (every pixel in one launch; the reference's tiles change no value)."""
+    return render_stokes_image_bricks_device(cfg, snapshot, bricks).cpu().numpy()
+
+
+__all__ = ["AcceleratedRenderConfig", "DIAGNOSTICS", "render_stokes_image_bricks", "render_stokes_image_bricks_device",
+           "render_tile_stokes_bricks"]

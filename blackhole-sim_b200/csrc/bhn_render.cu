@@ -1235,3 +1235,4 @@ int bhn_graph_destroy(bhn_graph *graph) {
 }  // extern "C"
 #include "bhn_learned.cuh"
 #include "bhn_grrt.cuh"
+#include "bhn_bricktrace.cuh"

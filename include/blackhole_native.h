@@ -358,6 +358,32 @@ int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, cons
                     const bhn_grrt_config *cfg, void *scratch, int64_t scratch_bytes, double *out, double *diag,
                     void *stream);
 
+/* ---- the reference's brick renderer (RK4 fixed step) ----------------------
+ * Replaces render_stokes_image_bricks / render_tile_stokes_bricks
+ * (python/blackhole_sim/accelerated_renderer.py:100-158): per pixel of one
+ * view (a crop = a tile) the camera ray, a fixed-step RK4 geodesic
+ * (kerr.py:306-313, 337-384) and integrate_stokes_from_bricks_trace: the
+ * coefficient brick sampled at each segment's midpoint (no sample outside the
+ * nonperiodic r / theta range), ds = length_cm * max(|d(r, theta, phi)|,
+ * 1e-14), an RK2 or exact Stokes step, the optical-depth cutoff, and
+ * non-finite results set to 0; FP64, one thread per ray.  (bhn_render_launch
+ * is the RK2, h = 0.02 r form of the same loop.)  coeffs: [nr][nt][np][11]
+ * float64; out: [rays][4] at view->out_offset; diag (optional): [rays][4] =
+ * optical depth, sampled segments, RK4 steps taken, BHN_RAY_* status.
+ * scratch: bhn_render_scratch_bytes(1). */
+typedef struct bhn_brick_trace_config {
+    double step;                 /* affine RK4 step (AcceleratedRenderConfig.step) */
+    double escape_radius;
+    double length_cm;            /* affine_to_length_cm (1.0 when the config leaves it unset) */
+    double max_optical_depth;
+    int32_t max_steps;
+    int32_t exact_step;          /* 1: stokes_step_exact, 0: RK2 */
+} bhn_brick_trace_config;
+int bhn_brick_trace_render(const double *coeffs, const double *r_grid, int32_t nr, const double *theta_grid,
+                           int32_t nt, const double *phi_grid, int32_t np, const bhn_view *view,
+                           const bhn_brick_trace_config *cfg, void *scratch, int64_t scratch_bytes, double *out,
+                           double *diag, void *stream);
+
 /* CUDA-graph form of bhn_render_launch: captures the queue reset and the
  * persistent launch once; bhn_graph_launch replays it on `stream`. */
 typedef struct bhn_graph bhn_graph;

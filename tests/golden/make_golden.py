@@ -421,10 +421,45 @@ def rgb_fixtures(pr) -> dict[str, np.ndarray]:
             "rgb_dark_in": dark, "rgb_dark_out": pr.stokes_to_rgb(dark)}
 
 
+def accel_fixtures(cb, acc, kerr, pt, grmhd) -> dict[str, np.ndarray]:
+    """accelerated_renderer.render_stokes_image_bricks (accelerated_renderer.py:
+    153-158) on a 5 x 4 image of a seeded 10 x 8 x 12 brick, float64 and
+    float32 coefficients, RK2 and exact Stokes steps, with a short cutoff run;
+    and render_tile_stokes_bricks on one tile."""
+    rng = np.random.default_rng(13)
+    r = np.geomspace(1.5, 40.0, 10)
+    theta = (np.arange(8) + 0.5) * math.pi / 8.0
+    phi = np.linspace(0.0, 2.0 * math.pi, 12, endpoint=False)
+    dens = np.exp(-((r[:, None, None] - 8.0) ** 2) / 8.0 - 4.0 * np.cos(theta)[None, :, None] ** 2) * np.ones((10, 8, 12))
+    coeffs = np.zeros((10, 8, 12, 11))
+    coeffs[..., :4] = dens[..., None] * np.array([1.0, 0.2, 0.1, 0.02]) * 1e-3
+    coeffs[..., 4:8] = 0.1 * coeffs[..., :4] * 10.0
+    coeffs[..., 8:] = dens[..., None] * rng.uniform(0.5, 1.5, (10, 8, 12, 3)) * 1e-2
+    cam = kerr.LocalCamera.from_degrees(r=30.0, inclination_degrees=70.0, fov_y_degrees=30.0)
+    snap = grmhd.GRMHDSnapshot(r=r, theta=theta, phi=phi, rho=dens, theta_e=np.ones_like(dens),
+                               pressure=dens, b_con=np.zeros(dens.shape + (4,)), u_con=np.zeros(dens.shape + (4,)),
+                               spin_a=0.9375)
+    out = {"acc_r": r, "acc_theta": theta, "acc_phi": phi, "acc_coeffs": coeffs, "acc_cam": np.array([cam.r, cam.theta, cam.phi, cam.fov_y_degrees])}
+    for dt in ("float64", "float32"):
+        bricks = cb.CoefficientBrickGrid(r, theta, phi, coeffs.astype(dt), 230e9, 0.9375, dt)
+        for exact in (False, True):
+            for max_tau in (30.0, 0.006):
+                cfg = acc.AcceleratedRenderConfig(width=5, height=4, camera=cam, step=0.1, max_steps=900,
+                                                  transfer=pt.PolarizedTransferConfig(use_exact_matrix_step=exact,
+                                                                                      affine_to_length_cm=2.0,
+                                                                                      max_optical_depth=max_tau))
+                out[f"acc_{dt}_{'exact' if exact else 'rk2'}_{'cut' if max_tau < 1 else 'full'}"] = \
+                    acc.render_stokes_image_bricks(cfg, snap, bricks)
+        cfg = acc.AcceleratedRenderConfig(width=5, height=4, camera=cam, step=0.1, max_steps=900)
+        tile = acc.RenderTile(level=0, y0=1, x0=2, x1=5, y1=3)
+        out[f"acc_{dt}_tile"] = acc.render_tile_stokes_bricks(cfg, snap, bricks, tile)
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/python")
-    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb")
+    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb,accel")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
@@ -457,6 +492,9 @@ def main() -> None:
     if not only or "grrt" in only:
         np.savez_compressed(HERE / "grrt.npz", **grrt_fixtures(grmhd, calibration, kerr, pr))
         print("wrote grrt.npz")
+    if not only or "accel" in only:
+        np.savez_compressed(HERE / "accel.npz", **accel_fixtures(cb, acc, kerr, pt, grmhd))
+        print("wrote accel.npz")
     if not only or "rgb" in only:
         np.savez_compressed(HERE / "stokes_rgb.npz", **rgb_fixtures(pr))
         print("wrote stokes_rgb.npz")

@@ -1,0 +1,117 @@
+"""The reference's own brick renderer (accelerated_renderer.render_stokes_image_bricks
+/ render_tile_stokes_bricks, python/blackhole_sim/accelerated_renderer.py:100-158:
+fixed-step RK4, trilinear brick samples, RK2 or exact Stokes steps): the oracle
+(oracle/bricktrace.py) and the GPU (bhn_brick_trace_render) against the
+reference's own 5 x 4 images of a seeded brick (tests/golden/accel.npz).
+
+The reference interpolates with float32 weights (its float32 grids under
+NumPy's promotion rules) while oracle and GPU do it in float64: pixels agree
+to 1e-6 relative (measured 3e-8)."""
+
+from __future__ import annotations
+
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+from oracle import bricktrace as B
+from oracle import oracle as O
+
+TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def golden():
+    with np.load(Path(__file__).parent / "golden" / "accel.npz") as z:
+        return {k: z[k] for k in z}
+
+
+def _grids(g):
+    return [g[k].astype(np.float32).astype(np.float64) for k in ("acc_r", "acc_theta", "acc_phi")]
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
+
+
+def _cases():
+    for dt in ("float64", "float32"):
+        for step in ("rk2", "exact"):
+            for cut in ("full", "cut"):
+                yield dt, step, cut
+
+
+@pytest.mark.parametrize("dt,step,cut", [c for c in _cases() if c[2] == "cut" or c[1] == "rk2"])
+def test_oracle_matches_reference(golden, dt, step, cut):
+    rg, tg, pg = _grids(golden)
+    cam = golden["acc_cam"]
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = 0.9375, cam[0], cam[1], cam[2]
+    v.fov_y_deg, v.roll_deg, v.width, v.height = cam[3], 0.0, 5, 4
+    coeffs = golden["acc_coeffs"].astype(dt).astype(np.float64)
+    ref = golden[f"acc_{dt}_{step}_{cut}"]
+    for px, py in ((0, 0), (2, 1), (4, 3)):
+        S, (tau, n) = B.trace_pixel_bricks(v, coeffs, rg, tg, pg, 0.1, 900, 220.0, length_cm=2.0, exact=step == "exact",
+                                           max_tau=30.0 if cut == "full" else 0.006, px=px, py=py)
+        assert n > 0 and _rel(S, ref[py, px]) <= TOL
+
+
+def _config(acc, cam, step, cut):
+    from blackhole_native import grrt
+
+    tr = grrt.PolarizedTransferConfig(use_exact_matrix_step=step == "exact", affine_to_length_cm=2.0,
+                                      max_optical_depth=30.0 if cut == "full" else 0.006)
+    return acc.AcceleratedRenderConfig(width=5, height=4, camera=grrt.LocalCamera(cam[0], cam[1], cam[2], cam[3]),
+                                       step=0.1, max_steps=900, transfer=tr)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dt,step,cut", list(_cases()))
+def test_gpu_matches_reference_image(golden, dt, step, cut):
+    from blackhole_native import accelerated as acc
+
+    bricks = SimpleNamespace(r=golden["acc_r"], theta=golden["acc_theta"], phi=golden["acc_phi"],
+                             coeffs=golden["acc_coeffs"].astype(dt))
+    snap = SimpleNamespace(spin_a=0.9375)
+    img, diag = acc.render_stokes_image_bricks_device(_config(acc, golden["acc_cam"], step, cut), snap, bricks,
+                                                      diagnostics=True)
+    img, diag = img.cpu().numpy(), diag.cpu().numpy()
+    ref = golden[f"acc_{dt}_{step}_{cut}"]
+    assert img.shape == (4, 5, 4) and np.all(np.isfinite(img))
+    for py in range(4):
+        for px in range(5):
+            assert _rel(img[py, px], ref[py, px]) <= TOL, (px, py)
+    if cut == "cut":
+        assert np.any(diag[..., 3] == 4) and np.all(diag[..., 0][diag[..., 3] == 4] >= 0.006)
+
+
+@pytest.mark.gpu
+def test_gpu_tile_and_oracle(golden):
+    """render_tile_stokes_bricks against the reference's tile, and a larger
+    image's pixels (with sampled-segment counts) against the oracle."""
+    from blackhole_native import accelerated as acc
+    from blackhole_native.tiles import RenderTile
+
+    cam = golden["acc_cam"]
+    bricks = SimpleNamespace(r=golden["acc_r"], theta=golden["acc_theta"], phi=golden["acc_phi"],
+                             coeffs=golden["acc_coeffs"].astype(np.float32))
+    snap = SimpleNamespace(spin_a=0.9375)
+    cfg = _config(acc, cam, "rk2", "full")
+    cfg = acc.AcceleratedRenderConfig(width=5, height=4, camera=cfg.camera, step=0.1, max_steps=900)
+    block = acc.render_tile_stokes_bricks(cfg, snap, bricks, RenderTile(level=0, y0=1, x0=2, x1=5, y1=3))
+    assert block.shape == (2, 3, 4) and _rel(block, golden["acc_float32_tile"]) <= TOL
+
+    big = acc.AcceleratedRenderConfig(width=24, height=16, camera=cfg.camera, step=0.1, max_steps=900,
+                                      transfer=_config(acc, cam, "rk2", "full").transfer)
+    img, diag = (t.cpu().numpy() for t in acc.render_stokes_image_bricks_device(big, snap, bricks, diagnostics=True))
+    rg, tg, pg = _grids(golden)
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = 0.9375, cam[0], cam[1], cam[2]
+    v.fov_y_deg, v.roll_deg, v.width, v.height = cam[3], 0.0, 24, 16
+    coeffs = golden["acc_coeffs"].astype(np.float32).astype(np.float64)
+    for px, py in ((0, 0), (11, 7), (23, 15)):
+        S, (tau, n) = B.trace_pixel_bricks(v, coeffs, rg, tg, pg, 0.1, 900, 220.0, length_cm=2.0, px=px, py=py)
+        assert n == diag[py, px, 1]
+        assert _rel(img[py, px], S) <= 1e-10 if np.any(S) else not np.any(img[py, px])
