@@ -642,28 +642,25 @@ struct Tracer32 {
                     const int64_t c00 = ((int64_t)ir * nt + it) * np;
                     const int64_t cells[4] = {c00, c00 + np, c00 + (int64_t)nt * np, c00 + (int64_t)nt * np + np};
                     const float wrt[4] = {owr * owt, owr * wt, wr * owt, wr * wt};
-                    float cf[11];
-#pragma unroll
-                    for (int k = 0; k < 11; ++k) cf[k] = 0.0f;
+                    // channels in pairs on the paired FP32 FMA (each lane one fmaf, same order)
+                    float2 c01 = make_float2(0.0f, 0.0f), c23 = c01, c45 = c01, c67 = c01, c89 = c01;
+                    float c10 = 0.0f;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const float4 *p0 = rec + 3 * (cells[q] + ip);
                         const float4 *p1 = rec + 3 * (cells[q] + ip1);
                         const float w0 = wrt[q] * owp, w1 = wrt[q] * wp;
+                        const float2 W0 = make_float2(w0, w0), W1 = make_float2(w1, w1);
                         const float4 a0 = __ldg(p0), b0 = __ldg(p0 + 1), c0 = __ldg(p0 + 2);
                         const float4 a1 = __ldg(p1), b1 = __ldg(p1 + 1), c1 = __ldg(p1 + 2);
-                        cf[0] = fmaf(w0, a0.x, fmaf(w1, a1.x, cf[0]));
-                        cf[1] = fmaf(w0, a0.y, fmaf(w1, a1.y, cf[1]));
-                        cf[2] = fmaf(w0, a0.z, fmaf(w1, a1.z, cf[2]));
-                        cf[3] = fmaf(w0, a0.w, fmaf(w1, a1.w, cf[3]));
-                        cf[4] = fmaf(w0, b0.x, fmaf(w1, b1.x, cf[4]));
-                        cf[5] = fmaf(w0, b0.y, fmaf(w1, b1.y, cf[5]));
-                        cf[6] = fmaf(w0, b0.z, fmaf(w1, b1.z, cf[6]));
-                        cf[7] = fmaf(w0, b0.w, fmaf(w1, b1.w, cf[7]));
-                        cf[8] = fmaf(w0, c0.x, fmaf(w1, c1.x, cf[8]));
-                        cf[9] = fmaf(w0, c0.y, fmaf(w1, c1.y, cf[9]));
-                        cf[10] = fmaf(w0, c0.z, fmaf(w1, c1.z, cf[10]));
+                        c01 = __ffma2_rn(W0, make_float2(a0.x, a0.y), __ffma2_rn(W1, make_float2(a1.x, a1.y), c01));
+                        c23 = __ffma2_rn(W0, make_float2(a0.z, a0.w), __ffma2_rn(W1, make_float2(a1.z, a1.w), c23));
+                        c45 = __ffma2_rn(W0, make_float2(b0.x, b0.y), __ffma2_rn(W1, make_float2(b1.x, b1.y), c45));
+                        c67 = __ffma2_rn(W0, make_float2(b0.z, b0.w), __ffma2_rn(W1, make_float2(b1.z, b1.w), c67));
+                        c89 = __ffma2_rn(W0, make_float2(c0.x, c0.y), __ffma2_rn(W1, make_float2(c1.x, c1.y), c89));
+                        c10 = fmaf(w0, c0.z, fmaf(w1, c1.z, c10));
                     }
+                    const float cf[11] = {c01.x, c01.y, c23.x, c23.y, c45.x, c45.y, c67.x, c67.y, c89.x, c89.y, c10};
                     // ds = L * max(|d(r, theta, phi)|, 1e-14) (accelerated_renderer.py:120-121)
                     const float dth = th1 - th0;
                     const float ds = C.L * fmaxf(sqrtf(fmaf(dr, dr, fmaf(dth, dth, dph * dph))), 1.0e-14f);
