@@ -84,22 +84,33 @@ def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagn
     """(h, w, 4) float64 Stokes image of the tile (default: the whole image)
     on the device, and (h, w, 4) diagnostics (columns ``DIAGNOSTICS``) when
     asked.  ``snapshot`` supplies the spin (``spin_a``)."""
-    L = _declare()
-    device = device or dev.require_cuda()
+    # host-side checks first: a bad call fails the same way with or without a GPU
     coeffs = np.asarray(bricks.coeffs)
-    shape = tuple(np.asarray(getattr(bricks, n)).size for n in ("r", "theta", "phi"))
+    host_grids = [_grid(getattr(bricks, n)) for n in ("r", "theta", "phi")]
+    shape = tuple(g.size for g in host_grids)
     if coeffs.shape != shape + (11,):
         raise ValueError(f"coeffs must have shape {shape + (11,)}; got {coeffs.shape}")
     if not np.all(np.isfinite(coeffs)):
         raise ValueError("coefficient brick contains non-finite values")
-    grids = [torch.as_tensor(_grid(getattr(bricks, n)), device=device) for n in ("r", "theta", "phi")]
-    d_coeffs = torch.as_tensor(np.ascontiguousarray(coeffs, dtype=np.float64), device=device)
-    cam = cfg.camera
     W, H = int(cfg.width), int(cfg.height)
     if W < 1 or H < 1:
         raise ValueError("image width and height must be positive")
+    if not (np.isfinite(cfg.step) and cfg.step > 0.0):
+        raise ValueError("step must be finite and positive")
+    if int(cfg.max_steps) < 0:
+        raise ValueError("max_steps must be non-negative")
     x0, y0, w, h = (0, 0, W, H) if tile is None else (int(tile.x0), int(tile.y0), int(tile.x1 - tile.x0),
                                                        int(tile.y1 - tile.y0))
+    if not (0 <= x0 and 0 <= y0 and w >= 0 and h >= 0 and x0 + w <= W and y0 + h <= H):
+        raise ValueError(f"tile ({x0}, {y0}, {w}x{h}) lies outside the {W}x{H} image")
+    L = _declare()
+    device = device or dev.require_cuda()
+    grids = [torch.as_tensor(g, device=device) for g in host_grids]
+    if w == 0 or h == 0:  # an empty tile: the reference's loop over no pixels
+        out = torch.zeros((h, w, 4), dtype=torch.float64, device=device)
+        return (out, torch.zeros_like(out)) if diagnostics else out
+    d_coeffs = torch.as_tensor(np.ascontiguousarray(coeffs, dtype=np.float64), device=device)
+    cam = cfg.camera
     v = _lib.ViewStruct()
     v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = float(snapshot.spin_a), float(cam.r), float(cam.theta), float(cam.phi)
     v.fov_y_deg, v.roll_deg = float(cam.fov_y_degrees), float(getattr(cam, "roll_degrees", 0.0))

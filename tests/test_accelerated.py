@@ -115,3 +115,104 @@ def test_gpu_tile_and_oracle(golden):
         S, (tau, n) = B.trace_pixel_bricks(v, coeffs, rg, tg, pg, 0.1, 900, 220.0, length_cm=2.0, px=px, py=py)
         assert n == diag[py, px, 1]
         assert _rel(img[py, px], S) <= 1e-10 if np.any(S) else not np.any(img[py, px])
+
+
+def _golden_bricks(golden, dt=np.float32):
+    return SimpleNamespace(r=golden["acc_r"], theta=golden["acc_theta"], phi=golden["acc_phi"],
+                           coeffs=golden["acc_coeffs"].astype(dt))
+
+
+def test_host_validation_before_any_device_work(golden):
+    """Bad bricks, configs and tiles raise ValueError on the host, GPU or not."""
+    from dataclasses import replace
+
+    from blackhole_native import accelerated as acc
+    from blackhole_native.tiles import RenderTile
+
+    snap = SimpleNamespace(spin_a=0.9375)
+    cfg = _config(acc, golden["acc_cam"], "rk2", "full")
+    good = _golden_bricks(golden)
+    bad_shape = SimpleNamespace(**{**vars(good), "coeffs": good.coeffs[:, :, :-1]})
+    with pytest.raises(ValueError, match="coeffs must have shape"):
+        acc.render_stokes_image_bricks(cfg, snap, bad_shape)
+    nonfinite = SimpleNamespace(**{**vars(good), "coeffs": good.coeffs.copy()})
+    nonfinite.coeffs[1, 1, 1, 4] = np.nan
+    with pytest.raises(ValueError, match="non-finite"):
+        acc.render_stokes_image_bricks(cfg, snap, nonfinite)
+    unsorted = SimpleNamespace(**{**vars(good), "r": good.r[::-1].copy()})
+    with pytest.raises(ValueError, match="strictly increasing"):
+        acc.render_stokes_image_bricks(cfg, snap, unsorted)
+    with pytest.raises(ValueError, match="step must be"):
+        acc.render_stokes_image_bricks(replace(cfg, step=0.0), snap, good)
+    with pytest.raises(ValueError, match="max_steps"):
+        acc.render_stokes_image_bricks(replace(cfg, max_steps=-1), snap, good)
+    with pytest.raises(ValueError, match="outside"):
+        acc.render_tile_stokes_bricks(cfg, snap, good, RenderTile(level=0, y0=0, x0=3, x1=6, y1=2))
+
+
+def test_c_abi_rejects_bad_arguments_before_device_work():
+    """bhn_brick_trace_render checks pointers, grid sizes and the config on
+    the host and returns BHN_ERR_VALUE with a message, launching nothing."""
+    import ctypes
+
+    from blackhole_native import _lib
+    from blackhole_native import accelerated as acc
+
+    L = acc._declare()
+    buf = (ctypes.c_double * 64)()
+    p = ctypes.addressof(buf)
+    v = _lib.ViewStruct()
+    c = acc.BrickTraceConfigStruct(step=0.1, escape_radius=220.0, length_cm=1.0, max_optical_depth=30.0, max_steps=10,
+                                   exact_step=0)
+
+    def call(nr=4, cfg=c, out=p):
+        return L.bhn_brick_trace_render(p, p, nr, p, 4, p, 4, ctypes.byref(v), ctypes.byref(cfg), p, 512, out, None,
+                                        None)
+
+    assert call(out=None) == 1 and b"missing" in L.bhn_last_error()
+    assert call(nr=1) == 1 and b"at least 2" in L.bhn_last_error()
+    for field, value, msg in (("step", 0.0, b"step"), ("step", float("nan"), b"step"), ("max_steps", -1, b"max_steps"),
+                              ("length_cm", float("inf"), b"finite")):
+        bad = acc.BrickTraceConfigStruct.from_buffer_copy(c)
+        setattr(bad, field, value)
+        assert call(cfg=bad) == 1 and msg in L.bhn_last_error(), field
+
+
+def test_config_struct_layout_matches_ctypes(tmp_path):
+    import ctypes
+    import shutil
+    import subprocess
+
+    from blackhole_native import accelerated as acc
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    include = Path(__file__).resolve().parents[1] / "include"
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "blackhole_native.h"\n'
+                   'int main(void){printf("%zu %zu %zu\\n", sizeof(bhn_brick_trace_config),'
+                   ' offsetof(bhn_brick_trace_config, max_steps), offsetof(bhn_brick_trace_config, exact_step));'
+                   ' return 0;}\n')
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", str(include), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    S = acc.BrickTraceConfigStruct
+    assert got == [ctypes.sizeof(S), S.max_steps.offset, S.exact_step.offset]
+
+
+@pytest.mark.gpu
+def test_gpu_edge_cases(golden):
+    """max_steps = 0 traces nothing (a zero image, status max_steps); an empty
+    tile gives an empty block, as the reference's loop over no pixels."""
+    from dataclasses import replace
+
+    from blackhole_native import accelerated as acc
+    from blackhole_native.tiles import RenderTile
+
+    snap = SimpleNamespace(spin_a=0.9375)
+    cfg = _config(acc, golden["acc_cam"], "rk2", "full")
+    img, diag = (t.cpu().numpy() for t in acc.render_stokes_image_bricks_device(
+        replace(cfg, max_steps=0), snap, _golden_bricks(golden), diagnostics=True))
+    assert not np.any(img) and not np.any(diag[..., :3]) and np.all(diag[..., 3] == 0)  # BHN_RAY_MAX_STEPS
+    block = acc.render_tile_stokes_bricks(cfg, snap, _golden_bricks(golden), RenderTile(level=0, y0=2, x0=1, x1=4, y1=2))
+    assert block.shape == (0, 3, 4)
