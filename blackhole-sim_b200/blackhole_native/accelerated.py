@@ -79,19 +79,25 @@ def _grid(g) -> np.ndarray:
     return np.ascontiguousarray(a)
 
 
-def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagnostics: bool = False,
-                                      device: torch.device | None = None):
-    """(h, w, 4) float64 Stokes image of the tile (default: the whole image)
-    on the device, and (h, w, 4) diagnostics (columns ``DIAGNOSTICS``) when
-    asked.  ``snapshot`` supplies the spin (``spin_a``)."""
-    # host-side checks first: a bad call fails the same way with or without a GPU
-    coeffs = np.asarray(bricks.coeffs)
-    host_grids = [_grid(getattr(bricks, n)) for n in ("r", "theta", "phi")]
-    shape = tuple(g.size for g in host_grids)
-    if coeffs.shape != shape + (11,):
-        raise ValueError(f"coeffs must have shape {shape + (11,)}; got {coeffs.shape}")
-    if not np.all(np.isfinite(coeffs)):
-        raise ValueError("coefficient brick contains non-finite values")
+class DeviceBricks:
+    """A ``CoefficientBrickGrid`` checked and uploaded once: float64
+    coefficients and grids on the device, for repeated renders."""
+
+    def __init__(self, bricks, device: torch.device | None = None):
+        coeffs = np.asarray(bricks.coeffs)
+        host_grids = [_grid(getattr(bricks, n)) for n in ("r", "theta", "phi")]
+        self.shape = tuple(g.size for g in host_grids)
+        if coeffs.shape != self.shape + (11,):
+            raise ValueError(f"coeffs must have shape {self.shape + (11,)}; got {coeffs.shape}")
+        if not np.all(np.isfinite(coeffs)):
+            raise ValueError("coefficient brick contains non-finite values")
+        self.device = device or dev.require_cuda()
+        self.grids = [torch.as_tensor(g, device=self.device) for g in host_grids]
+        self.coeffs = torch.as_tensor(np.ascontiguousarray(coeffs, dtype=np.float64), device=self.device)
+
+
+def _view_and_config(cfg, snapshot, tile):
+    """The bhn_view (camera, crop) and bhn_brick_trace_config of one call, checked on the host."""
     W, H = int(cfg.width), int(cfg.height)
     if W < 1 or H < 1:
         raise ValueError("image width and height must be positive")
@@ -103,13 +109,6 @@ def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagn
                                                        int(tile.y1 - tile.y0))
     if not (0 <= x0 and 0 <= y0 and w >= 0 and h >= 0 and x0 + w <= W and y0 + h <= H):
         raise ValueError(f"tile ({x0}, {y0}, {w}x{h}) lies outside the {W}x{H} image")
-    L = _declare()
-    device = device or dev.require_cuda()
-    grids = [torch.as_tensor(g, device=device) for g in host_grids]
-    if w == 0 or h == 0:  # an empty tile: the reference's loop over no pixels
-        out = torch.zeros((h, w, 4), dtype=torch.float64, device=device)
-        return (out, torch.zeros_like(out)) if diagnostics else out
-    d_coeffs = torch.as_tensor(np.ascontiguousarray(coeffs, dtype=np.float64), device=device)
     cam = cfg.camera
     v = _lib.ViewStruct()
     v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = float(snapshot.spin_a), float(cam.r), float(cam.theta), float(cam.phi)
@@ -124,14 +123,33 @@ def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagn
     c.length_cm = float(getattr(t, "affine_to_length_cm", None) or 1.0)  # accelerated_renderer.py:146
     c.max_optical_depth, c.max_steps = float(t.max_optical_depth), int(cfg.max_steps)
     c.exact_step = int(bool(t.use_exact_matrix_step))
+    return v, c, (h, w)
+
+
+def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagnostics: bool = False,
+                                      device: torch.device | None = None):
+    """(h, w, 4) float64 Stokes image of the tile (default: the whole image)
+    on the device, and (h, w, 4) diagnostics (columns ``DIAGNOSTICS``) when
+    asked.  ``snapshot`` supplies the spin (``spin_a``); ``bricks`` is a
+    ``CoefficientBrickGrid``-like object or a ``DeviceBricks``."""
+    # host-side checks first: a bad call fails the same way with or without a GPU
+    v, c, (h, w) = _view_and_config(cfg, snapshot, tile)
+    if not isinstance(bricks, DeviceBricks):
+        bricks = DeviceBricks(bricks, device)
+    device = bricks.device
+    if w == 0 or h == 0:  # an empty tile: the reference's loop over no pixels
+        out = torch.zeros((h, w, 4), dtype=torch.float64, device=device)
+        return (out, torch.zeros_like(out)) if diagnostics else out
+    L = _declare()
     nbytes = int(L.bhn_render_scratch_bytes(1))
     scratch = torch.empty(nbytes // 8 + 64, dtype=torch.float64, device=device)
     sp = (dev.ptr(scratch) + 255) & ~255
     out = torch.empty((h, w, 4), dtype=torch.float64, device=device)
     diag = torch.empty((h, w, 4), dtype=torch.float64, device=device) if diagnostics else None
-    _lib.check(L.bhn_brick_trace_render(dev.ptr(d_coeffs), dev.ptr(grids[0]), shape[0], dev.ptr(grids[1]), shape[1],
-                                        dev.ptr(grids[2]), shape[2], ctypes.byref(v), ctypes.byref(c), sp, nbytes,
-                                        dev.ptr(out), dev.ptr(diag), dev.stream_ptr()))
+    g, n = bricks.grids, bricks.shape
+    _lib.check(L.bhn_brick_trace_render(dev.ptr(bricks.coeffs), dev.ptr(g[0]), n[0], dev.ptr(g[1]), n[1], dev.ptr(g[2]),
+                                        n[2], ctypes.byref(v), ctypes.byref(c), sp, nbytes, dev.ptr(out),
+                                        dev.ptr(diag), dev.stream_ptr()))
     return (out, diag) if diagnostics else out
 
 
@@ -146,5 +164,5 @@ def render_stokes_image_bricks(cfg, snapshot, bricks) -> np.ndarray:
     return render_stokes_image_bricks_device(cfg, snapshot, bricks).cpu().numpy()
 
 
-__all__ = ["AcceleratedRenderConfig", "DIAGNOSTICS", "render_stokes_image_bricks", "render_stokes_image_bricks_device",
+__all__ = ["AcceleratedRenderConfig", "DIAGNOSTICS", "DeviceBricks", "render_stokes_image_bricks", "render_stokes_image_bricks_device",
            "render_tile_stokes_bricks"]
