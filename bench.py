@@ -18,7 +18,8 @@ precompute (coefficient bricks from a 256 x 128 x 256 seeded snapshot, cells/s)
 and grrt (the physical polarized renderer's default 160 x 90 image, pixels/s),
 whose lines carry an FP64 exp() roofline measured in the same run; learned
 (time to an image at 1e-3 Stokes-I error: the learned step size against plain
-RK2 and the step-doubling controller).
+RK2 and the step-doubling controller); bricks (the reference's own fixed-step
+RK4 brick renderer, its default 160 x 90 image, pixels/s, FP64 roofline).
 For N > 1 the job runs as torchrun ranks, one full image per rank (replicas:
 rays are independent and the path has no exchange step).
 """
@@ -807,6 +808,146 @@ def grrt_cpu_baseline(snap, scaling, cfg, target_s: float) -> dict:
                       f"({segs} emitting segments) in {dt:.2f} s"}
 
 
+# The reference's own brick renderer (accelerated_renderer.render_stokes_image_bricks)
+BRICKS_BRICK = dict(nr=128, ntheta=64, nphi=128, spin_a=0.9375, seed=0)
+BRICKS_PROFILE = REPO / "profiles" / "brick_trace_kernel_default_image.md"
+# FP64 FLOP of the fixed-step method (a multiply or add = 1, an FMA = 2, a
+# divide / sqrt / sincos = 1): an RK4 step is four right-hand sides of 129
+# (metric, three reciprocals, both quotient-rule derivatives) plus the stage
+# arguments and the update; a sampled segment adds the midpoint, the weights,
+# the 11-channel trilinear sample (7 lerps x 11 x 3), ds, the Stokes RK2 step
+# and the optical depth.
+FP64_FLOP_PER_RK4_STEP = 577
+FP64_FLOP_PER_SEGMENT = 336
+
+
+def bench_bricks(args) -> dict | None:
+    """The reference's brick renderer (accelerated_renderer.py:100-158): one
+    step = its default 160 x 90 image (camera r = 55 M, i = 65 deg, FOV 32
+    deg, RK4 step 0.06, 5000 steps, RK2 Stokes steps) of a seeded
+    128 x 64 x 128 x 11 float32 torus brick, FP64, one thread per ray."""
+    from types import SimpleNamespace
+
+    import torch
+
+    from blackhole_native import accelerated as acc
+    from blackhole_native import bricks
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    init_dist(world, "nccl")
+    stream = torch.cuda.current_stream(device)
+    B = BRICKS_BRICK
+    b = bricks.torus_brick(B["nr"], B["ntheta"], B["nphi"], spin_a=B["spin_a"], seed=B["seed"], dtype=np.float32)
+    grid = SimpleNamespace(r=b.r, theta=b.theta, phi=b.phi, coeffs=b.coeffs)
+    snap = SimpleNamespace(spin_a=B["spin_a"])
+    cfg = acc.AcceleratedRenderConfig()
+    if args.side:  # a larger or smaller image of the same scene
+        cfg = acc.AcceleratedRenderConfig(width=args.side, height=max(1, round(args.side * 9 / 16)))
+    db = acc.DeviceBricks(grid, device)
+    pixels = cfg.width * cfg.height
+    img, diag = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True)
+    torch.cuda.synchronize(device)
+    d = diag.cpu().numpy()
+    steps, segments = float(d[..., 2].sum()), float(d[..., 1].sum())
+    peaks = fp64_peaks(device, stream)
+    for _ in range(args.warmup):
+        acc.render_stokes_image_bricks_device(cfg, snap, db)
+    clocks = ClockSampler(_uuid(device)).start()
+    time.sleep(0.3)
+    barrier(world)
+    outs = []
+    per = timed_launches(lambda: outs.append(acc.render_stokes_image_bricks_device(cfg, snap, db)), args.steps,
+                         stream, device)
+    barrier(world)
+    clk = clocks.stop()
+    assert all(torch.equal(o, img) for o in outs), "images differ between launches"
+    t_max = max_over_ranks(sum(per), world, device)
+    value = sum_over_ranks(pixels * args.steps, world, device) / (t_max * 1e-3)
+
+    e2e = None
+    if not args.no_e2e:  # public API: host brick in (float32, converted and uploaded), host image out
+        ke = max(1, min(args.steps, 3))
+        barrier(world)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        a0.record(stream)
+        for _ in range(ke):
+            host = acc.render_stokes_image_bricks(cfg, snap, grid)
+        a1.record(stream)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        te = max_over_ranks(a0.elapsed_time(a1), world, device)
+        assert np.array_equal(host, img.cpu().numpy()), "public-API image differs from the device launch"
+        h2d = int(b.coeffs.size * 8 + (b.r.size + b.theta.size + b.phi.size) * 8)
+        e2e = {"value": sum_over_ranks(pixels * ke, world, device) / (te * 1e-3), "unit": "pixels/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(pixels * 4 * 8), "ms_per_step": te / ke,
+               "api": "render_stokes_image_bricks"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = bricks_cpu_baseline(grid, snap, cfg, args.cpu_seconds)
+    per_mean = statistics.mean(per)
+    flops = FP64_FLOP_PER_RK4_STEP * steps + FP64_FLOP_PER_SEGMENT * segments
+    achieved = flops / (per_mean * 1e-3) / 1e12
+    line = {
+        "metric": "pixels/s", "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"reference brick renderer (render_stokes_image_bricks), {cfg.width}x{cfg.height} "
+                               "pixels, camera r=55M i=65deg FOV 32deg, RK4 step 0.06, 5000 steps, RK2 Stokes "
+                               f"steps, seeded {B['nr']}x{B['ntheta']}x{B['nphi']}x11 float32 torus brick",
+                   "pixels_per_step": pixels, "rk4_steps_per_step": steps, "sampled_segments_per_step": segments,
+                   "l2": "brick (92 MB of float64 coefficients) resident in L2 between launches; the rays read "
+                         "at most a few cells per step",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": e2e, "gpu_launches": args.steps * 2,  # setup_views_kernel + brick_trace_kernel
+        "clocks": clk,
+        "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(peaks["fma_tflops"], 2),
+                     "unit": "TFLOP/s", "frac": round(achieved / peaks["fma_tflops"], 4),
+                     "traffic": profiled_traffic(BRICKS_PROFILE),
+                     "peak_source": "measured in this run (bhn_fp64_peak_probe FMA chains)",
+                     "kernel": "brick_trace_kernel",
+                     "algorithmic_flops_per_launch": flops,
+                     "flop_per_rk4_step": FP64_FLOP_PER_RK4_STEP, "flop_per_segment": FP64_FLOP_PER_SEGMENT},
+        "cpu_baseline": cpu,
+        "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
+    }
+    if world > 1:
+        import torch.distributed as td
+
+        td.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def bricks_cpu_baseline(grid, snap, cfg, target_s: float) -> dict:
+    """The float64 oracle (oracle/bricktrace.py, one core) on pixels of the image's middle row."""
+    sys.path.insert(0, str(REPO))
+    from oracle import bricktrace as OB
+    from oracle import oracle as O
+
+    cam = cfg.camera
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = snap.spin_a, cam.r, cam.theta, cam.phi
+    v.fov_y_deg, v.roll_deg, v.width, v.height = cam.fov_y_degrees, cam.roll_degrees, cfg.width, cfg.height
+    rg, tg, pg = (np.asarray(g, dtype=np.float32).astype(np.float64) for g in (grid.r, grid.theta, grid.phi))
+    coeffs = np.asarray(grid.coeffs, dtype=np.float64)
+    t0 = time.perf_counter()
+    n = segs = 0
+    py = cfg.height // 2
+    while n < cfg.width and (n == 0 or time.perf_counter() - t0 < target_s):
+        px = (cfg.width // 2 + n) % cfg.width
+        _, (_, k) = OB.trace_pixel_bricks(v, coeffs, rg, tg, pg, cfg.step, cfg.max_steps, cfg.escape_radius,
+                                          length_cm=1.0, px=px, py=py)
+        n += 1
+        segs += k
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "pixels/s", "cores": 1, "kind": "port",
+            "sample": f"float64 oracle (oracle/bricktrace.py, one core): {n} pixels of the middle row "
+                      f"({segs} sampled segments) in {dt:.2f} s"}
+
+
 def _scaled_traffic(summary: Path, scale: float) -> float | None:
     t = profiled_traffic(summary)
     return None if t is None else t * scale
@@ -937,14 +1078,16 @@ def main(argv=None) -> int:
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")
     ap.add_argument("--tune", action="store_true", help="run the launch-shape autotuner on the workload and exit")
-    ap.add_argument("--workload", choices=["image", "views", "precompute", "grrt", "learned"], default="image",
+    ap.add_argument("--workload", choices=["image", "views", "precompute", "grrt", "learned", "bricks"],
+                    default="image",
                     help="image: the 1024x1024 single view (default); views: many uneven views in one launch; "
                          "precompute: coefficient bricks from a snapshot; grrt: the physical polarized renderer; "
-                         "learned: time to an image at 1e-3, learned step size against plain RK2")
+                         "learned: time to an image at 1e-3, learned step size against plain RK2; bricks: the "
+                         "reference's own brick renderer (fixed-step RK4)")
     ap.add_argument("--n-views", type=int, default=256)
     ap.add_argument("--side", type=int, default=0,
-                    help="profiling only: image workload side x side rays; precompute nr = side; grrt image "
-                         "side x side*9/16")
+                    help="profiling only: image workload side x side rays; precompute nr = side; grrt and "
+                         "bricks image side x side*9/16")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, whatever is asked
     if args.impl == "reference":
@@ -957,6 +1100,8 @@ def main(argv=None) -> int:
         line = bench_grrt(args)
     elif args.workload == "learned":
         line = bench_learned(args)
+    elif args.workload == "bricks":
+        line = bench_bricks(args)
     else:
         line = bench_ours(args)
     if line is not None:
