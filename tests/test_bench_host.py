@@ -1,0 +1,40 @@
+"""bench.py's host-side pieces that need no GPU: the CPU-baseline leg of the
+brick-renderer workload (the oracle on a bounded sample) and its workload
+constants."""
+
+from __future__ import annotations
+
+import json
+import subprocess
+import sys
+from pathlib import Path
+from types import SimpleNamespace
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parents[1]
+
+
+def test_bricks_cpu_baseline_contract():
+    sys.path.insert(0, str(REPO))
+    import bench
+    from blackhole_native import accelerated as acc
+    from blackhole_native import bricks
+
+    b = bricks.torus_brick(16, 8, 16, spin_a=0.9375, seed=0, dtype=np.float32)
+    grid = SimpleNamespace(r=b.r, theta=b.theta, phi=b.phi, coeffs=b.coeffs)
+    cfg = acc.AcceleratedRenderConfig(width=8, height=4, max_steps=300)
+    out = bench.bricks_cpu_baseline(grid, SimpleNamespace(spin_a=0.9375), cfg, target_s=0.2)
+    assert set(out) == {"value", "unit", "cores", "kind", "sample"}
+    assert out["unit"] == "pixels/s" and out["cores"] == 1 and out["kind"] == "port" and out["value"] > 0
+    assert "oracle/bricktrace.py" in out["sample"]
+
+
+def test_bench_lists_the_bricks_workload():
+    out = subprocess.run([sys.executable, str(REPO / "bench.py"), "--help"], capture_output=True, text=True,
+                         check=True).stdout
+    assert "bricks" in out and "--workload" in out
+    import bench
+
+    assert bench.FP64_FLOP_PER_RK4_STEP > 4 * 100 and bench.FP64_FLOP_PER_SEGMENT > 7 * 11 * 3
+    json.dumps(bench.BRICKS_BRICK)
