@@ -31,6 +31,8 @@ __global__ void __launch_bounds__(128) brick_trace_kernel(const BrickTraceParams
     const ViewDev &v = *P.view;
     const int64_t rays = (int64_t)v.crop_w * v.crop_h;
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ AxisHints hints;  // the brick axes' first-guess parameters (the whole block)
+    load_axis_hints(hints, P.rg, P.nr, P.tg, P.nt, P.pg, P.np);
     if (r >= rays) return;
     const int px = v.x0 + (int)(r % v.crop_w), py = v.y0 + (int)(r / v.crop_w);
     double S[4] = {0.0, 0.0, 0.0, 0.0};
@@ -53,8 +55,8 @@ __global__ void __launch_bounds__(128) brick_trace_kernel(const BrickTraceParams
             }
             if (!stop_transfer) {
                 double c[11];
-                if (sample_one_exact(P.coeffs, P.rg, P.nr, P.tg, P.nt, P.pg, P.np, 0.5 * (y[0] + yn[0]),
-                                     0.5 * (y[1] + yn[1]), 0.5 * (y[2] + yn[2]), c)) {
+                if (sample_one_hinted(P.coeffs, P.rg, P.nr, P.tg, P.nt, P.pg, P.np, hints, 0.5 * (y[0] + yn[0]),
+                                      0.5 * (y[1] + yn[1]), 0.5 * (y[2] + yn[2]), c)) {
                     const double dr = yn[0] - y[0], dth = yn[1] - y[1], dph = yn[2] - y[2];
                     const double dl = sqrt((dr * dr + dth * dth) + dph * dph);
                     const double ds = fmax(P.length_cm * fmax(dl, 1.0e-14), 0.0);

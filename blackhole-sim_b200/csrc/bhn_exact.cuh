@@ -64,14 +64,9 @@ __device__ __forceinline__ void bracket_phi_exact(const double *g, int n, double
     w = sub(pp, g[lo]) / den;
 }
 
-// lib.rs:171-208 / native_kernels.py:164-186
-__device__ __forceinline__ bool sample_one_exact(const double *__restrict__ coeffs, const double *rg, int nr,
-                                                 const double *tg, int nt, const double *pg, int np, double r,
-                                                 double th, double ph, double out[11]) {
-    int r0, t0, p0, p1;
-    double wr, wt, wp;
-    if (!bracket_linear_exact(rg, nr, r, r0, wr) || !bracket_linear_exact(tg, nt, th, t0, wt)) return false;
-    bracket_phi_exact(pg, np, ph, p0, p1, wp);
+// The trilinear blend of native_kernels.py:180-186: phi lerps, then theta, then r.
+__device__ __forceinline__ bool lerp_cells(const double *__restrict__ coeffs, int nt, int np, int r0, int t0, int p0,
+                                           int p1, double wr, double wt, double wp, double out[11]) {
     const int r1 = r0 + 1, t1 = t0 + 1;
     auto off = [&](int ir, int it, int ip) { return ((((int64_t)ir * nt + it) * np) + ip) * 11; };
     const double *c000 = coeffs + off(r0, t0, p0), *c001 = coeffs + off(r0, t0, p1);
@@ -90,6 +85,122 @@ __device__ __forceinline__ bool sample_one_exact(const double *__restrict__ coef
         out[c] = add(mul(owr, cc0), mul(wr, cc1));
     }
     return true;
+}
+
+// First-guess parameters of the three brick axes (r, theta, phi), classified
+// once per block by its first warp: uniform when every knot lies within a
+// quarter cell of g0 + k d, geometric when within a quarter cell of
+// g0 exp(k dl), else binary search (the rule of build_tables_kernel).
+struct AxisHints {
+    int kind[3];
+    double off[3], inv[3];
+};
+
+__device__ __forceinline__ void classify_axis_warp(const double *g, int n, int lane, int &kind, double &off,
+                                                   double &inv) {
+    kind = kSearch;
+    off = inv = 0.0;
+    const double d = (g[n - 1] - g[0]) / (n - 1);
+    double dev = 0.0;
+    for (int k = lane; k < n; k += 32) dev = fmax(dev, fabs(g[k] - (g[0] + k * d)));
+    for (int o = 16; o > 0; o >>= 1) dev = fmax(dev, __shfl_xor_sync(0xffffffffu, dev, o));
+    if (dev <= 0.25 * d) {
+        kind = kUniform;
+        inv = 1.0 / d;
+        off = g[0] * inv;
+        return;
+    }
+    if (!(g[0] > 0.0)) return;
+    const double dl = log(g[n - 1] / g[0]) / (n - 1);
+    double devl = 0.0;
+    for (int k = lane; k < n; k += 32) devl = fmax(devl, fabs(log(g[k] / g[0]) - k * dl));
+    for (int o = 16; o > 0; o >>= 1) devl = fmax(devl, __shfl_xor_sync(0xffffffffu, devl, o));
+    if (devl <= 0.25 * dl) {
+        kind = kGeometric;
+        inv = 1.0 / dl;
+        off = log(g[0]) * inv;
+    }
+}
+
+// Every thread of the block must call this (it synchronises the block); the
+// block needs at least one full warp.  NaN or unsorted knots classify as
+// search, which is always exact.
+__device__ __forceinline__ void load_axis_hints(AxisHints &h, const double *rg, int nr, const double *tg, int nt,
+                                                const double *pg, int np) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        for (int a = 0; a < 3; ++a) {
+            int kind;
+            double off, inv;
+            classify_axis_warp(a == 0 ? rg : (a == 1 ? tg : pg), a == 0 ? nr : (a == 1 ? nt : np), lane, kind, off,
+                               inv);
+            if (!(isfinite(off) && isfinite(inv))) kind = kSearch;
+            if (lane == 0) {
+                h.kind[a] = kind;
+                h.off[a] = off;
+                h.inv[a] = inv;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// bracket_linear_exact with the cell found from the axis hint: the guess is
+// clamped and then fixed up against the knots, which gives
+// searchsorted(side="right") - 1 exactly for any sorted grid.
+__device__ __forceinline__ bool bracket_linear_hinted(const double *g, int n, double x, int kind, double off,
+                                                      double inv, int &i0, double &w) {
+    if (x < g[0] || x > g[n - 1]) return false;
+    if (x == g[n - 1]) {
+        i0 = n - 2;
+        w = 1.0;
+        return true;
+    }
+    const int lo = x == x ? locate_linear(g, n, x, kind, off, inv) : n - 2;  // NaN: the search's answer
+    double den = sub(g[lo + 1], g[lo]);
+    if (den < 1.0e-300) den = 1.0e-300;
+    i0 = lo;
+    w = sub(x, g[lo]) / den;
+    return true;
+}
+
+// bracket_phi_exact with the hinted cell search.
+__device__ __forceinline__ void bracket_phi_hinted(const double *g, int n, double phi, int kind, double off,
+                                                   double inv, int &i0, int &i1, double &w) {
+    double p = wrap_phi(phi, g[0]);
+    const int lo = (p >= g[0]) ? locate_phi(g, n, p, kind, off, inv) : n - 1;  // below g0 or NaN: the search's answer
+    int hi_i = (lo + 1) % n;
+    double hi = hi_i > lo ? g[hi_i] : add(g[0], kTwoPi);
+    double pp = p >= g[lo] ? p : add(p, kTwoPi);
+    double den = sub(hi, g[lo]);
+    if (den < 1.0e-300) den = 1.0e-300;
+    i0 = lo;
+    i1 = hi_i;
+    w = sub(pp, g[lo]) / den;
+}
+
+// lib.rs:171-208 / native_kernels.py:164-186
+__device__ __forceinline__ bool sample_one_exact(const double *__restrict__ coeffs, const double *rg, int nr,
+                                                 const double *tg, int nt, const double *pg, int np, double r,
+                                                 double th, double ph, double out[11]) {
+    int r0, t0, p0, p1;
+    double wr, wt, wp;
+    if (!bracket_linear_exact(rg, nr, r, r0, wr) || !bracket_linear_exact(tg, nt, th, t0, wt)) return false;
+    bracket_phi_exact(pg, np, ph, p0, p1, wp);
+    return lerp_cells(coeffs, nt, np, r0, t0, p0, p1, wr, wt, wp, out);
+}
+
+// sample_one_exact with the hinted brackets (same cells, weights and values).
+__device__ __forceinline__ bool sample_one_hinted(const double *__restrict__ coeffs, const double *rg, int nr,
+                                                  const double *tg, int nt, const double *pg, int np,
+                                                  const AxisHints &h, double r, double th, double ph, double out[11]) {
+    int r0, t0, p0, p1;
+    double wr, wt, wp;
+    if (!bracket_linear_hinted(rg, nr, r, h.kind[0], h.off[0], h.inv[0], r0, wr) ||
+        !bracket_linear_hinted(tg, nt, th, h.kind[1], h.off[1], h.inv[1], t0, wt))
+        return false;
+    bracket_phi_hinted(pg, np, ph, h.kind[2], h.off[2], h.inv[2], p0, p1, wp);
+    return lerp_cells(coeffs, nt, np, r0, t0, p0, p1, wr, wt, wp, out);
 }
 
 }  // namespace bhn

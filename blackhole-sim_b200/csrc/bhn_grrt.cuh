@@ -143,6 +143,8 @@ __global__ void __launch_bounds__(128) grrt_init_kernel(const TraceParams P, dou
 
 __global__ void __launch_bounds__(128) grrt_trace_kernel(const TraceParams P) {
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ AxisHints hints;  // the snapshot axes' first-guess parameters (the whole block)
+    load_axis_hints(hints, P.rg, P.nr, P.tg, P.nt, P.pg, P.np);
     if (r >= P.W.rays) return;
     GrrtRay &R = P.W.ray[r];
     R.count = 0;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(128) grrt_trace_kernel(const TraceParams P) {
         const double mpr = 0.5 * (y[3] + yn[3]), mpth = 0.5 * (y[4] + yn[4]);
         double f[11];
         const bool inside = isfinite(mr) && isfinite(mth) && isfinite(mph) &&
-                            sample_one_exact(P.fields, P.rg, P.nr, P.tg, P.nt, P.pg, P.np, mr, mth, mph, f);
+                            sample_one_hinted(P.fields, P.rg, P.nr, P.tg, P.nt, P.pg, P.np, hints, mr, mth, mph, f);
         // grmhd.py:119-120: rho > 0, Theta_e > 0, finite u
         if (inside && f[0] > 0.0 && f[1] > 0.0 && isfinite(f[7]) && isfinite(f[8]) && isfinite(f[9]) &&
             isfinite(f[10])) {
