@@ -164,5 +164,103 @@ def render_stokes_image_bricks(cfg, snapshot, bricks) -> np.ndarray:
     return render_stokes_image_bricks_device(cfg, snapshot, bricks).cpu().numpy()
 
 
-__all__ = ["AcceleratedRenderConfig", "DIAGNOSTICS", "DeviceBricks", "render_stokes_image_bricks", "render_stokes_image_bricks_device",
+@dataclass(frozen=True)
+class ProgressiveFrame:
+    """accelerated_renderer.py:51-56."""
+
+    level: int
+    width: int
+    height: int
+    stokes: np.ndarray
+
+
+def render_progressive_stokes_bricks(cfg, snapshot, bricks) -> list[ProgressiveFrame]:
+    """accelerated_renderer.py:161-166 on the GPU: one frame per progressive
+    level (tiles.progressive_levels), coarsest first; the brick is uploaded once."""
+    from dataclasses import replace
+
+    from .tiles import progressive_levels
+
+    db = bricks if isinstance(bricks, DeviceBricks) else None
+    frames = []
+    for level, w, h in progressive_levels(cfg.width, cfg.height, min_width=cfg.progressive_min_width):
+        level_cfg = replace(cfg, width=w, height=h)
+        if db is None:  # host-side checks of the first level's call come before the upload
+            _view_and_config(level_cfg, snapshot, None)
+            db = DeviceBricks(bricks)
+        frames.append(ProgressiveFrame(level=level, width=w, height=h,
+                                       stokes=render_stokes_image_bricks_device(level_cfg, snapshot, db).cpu().numpy()))
+    return frames
+
+
+def sample_coefficient_brick(bricks, r: float, theta: float, phi: float) -> np.ndarray | None:
+    """accelerated_renderer.py:73-97: the 11 coefficients at one point, or None
+    outside the brick's nonperiodic r / theta range; through the plugin
+    sampler ``sample_brick_trilinear`` (float64 weights on the brick's grid
+    values)."""
+    from .kernels import sample_brick_trilinear
+
+    grids = [_grid(getattr(bricks, n)) for n in ("r", "theta", "phi")]
+    coeffs = np.asarray(bricks.coeffs, dtype=np.float64).ravel()
+    out = np.asarray(sample_brick_trilinear(coeffs, *grids, [float(r), float(theta), float(phi)]), dtype=np.float64)
+    return None if not np.all(np.isfinite(out)) else out
+
+
+@dataclass(frozen=True)
+class ImageRegressionMetrics:
+    """webgpu_regression.py:27-36."""
+
+    max_abs: float
+    mean_abs: float
+    rmse: float
+    psnr_db: float
+    sha256: str
+
+    @property
+    def passed_default(self) -> bool:
+        return self.max_abs <= 0.035 and self.mean_abs <= 0.006
+
+
+def image_metrics(candidate, reference) -> ImageRegressionMetrics:
+    """webgpu_regression.py:39-48 (host arithmetic on two images)."""
+    import hashlib
+
+    a = np.asarray(candidate, dtype=float)
+    b = np.asarray(reference, dtype=float)
+    if a.shape != b.shape:
+        raise ValueError(f"shape mismatch: {a.shape} vs {b.shape}")
+    diff = np.abs(a - b)
+    rmse = float(np.sqrt(np.mean((a - b) ** 2)))
+    psnr = float(20.0 * np.log10(1.0 / max(rmse, 1.0e-300)))
+    digest = hashlib.sha256(np.asarray(candidate, dtype=np.float32).tobytes()).hexdigest()
+    return ImageRegressionMetrics(float(np.max(diff)), float(np.mean(diff)), rmse, psnr, digest)
+
+
+@dataclass(frozen=True)
+class SmallRegressionResult:
+    """accelerated_renderer.py:59-63."""
+
+    metrics: ImageRegressionMetrics
+    reference: np.ndarray
+    candidate: np.ndarray
+
+
+def compare_reference_vs_bricks(reference, candidate) -> SmallRegressionResult:
+    """accelerated_renderer.py:169-171: the images' tone-mapped difference."""
+    from .grrt import stokes_to_rgb
+
+    metrics = image_metrics(stokes_to_rgb(candidate), stokes_to_rgb(reference))
+    return SmallRegressionResult(metrics=metrics, reference=np.asarray(reference), candidate=np.asarray(candidate))
+
+
+def save_progressive_npz(frame: ProgressiveFrame, path) -> None:
+    """accelerated_renderer.py:178-179."""
+    from .grrt import save_stokes_npz
+
+    save_stokes_npz(frame.stokes, path)
+
+
+__all__ = ["AcceleratedRenderConfig", "DIAGNOSTICS", "DeviceBricks", "ImageRegressionMetrics", "ProgressiveFrame",
+           "SmallRegressionResult", "compare_reference_vs_bricks", "image_metrics", "render_progressive_stokes_bricks",
+           "sample_coefficient_brick", "save_progressive_npz", "render_stokes_image_bricks", "render_stokes_image_bricks_device",
            "render_tile_stokes_bricks"]

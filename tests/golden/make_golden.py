@@ -456,15 +456,50 @@ def accel_fixtures(cb, acc, kerr, pt, grmhd) -> dict[str, np.ndarray]:
     return out
 
 
+def accel_regression_fixtures(grmhd, calibration, cb, acc, pr, physics) -> dict[str, np.ndarray]:
+    """test_accelerated_renderer.py:17-78 as data: the analytic GRMHD torus
+    (generate_analytic_grmhd_torus(0.55, 8, 6, 6)), the Sgr A* scaling at
+    Mdot 1e-8, its float32 coefficient brick (precompute_coefficient_bricks),
+    the 3 x 2 physical and brick renders with compare_reference_vs_bricks'
+    metrics, the progressive frames of an 8 x 6 image and one brick sample."""
+    snap = grmhd.generate_analytic_grmhd_torus(spin_a=0.55, nr=8, ntheta=6, nphi=6)
+    scaling = calibration.PhysicalScaling.from_mdot(physics.BlackHoleSystem.sgr_a_star(0.55), 1e-8)
+    bricks = cb.precompute_coefficient_bricks(snap, scaling, nu_hz=230e9, dtype="float32", stride=1)
+    out = {f"snap_{k}": np.asarray(getattr(snap, k)) for k in
+           ("r", "theta", "phi", "rho", "theta_e", "pressure", "b_con", "u_con", "spin_a")}
+    for k in ("mass_bh_g", "distance_cm", "rho_cgs_per_code", "b_gauss_per_code",
+              "ion_to_electron_temperature_ratio", "mean_molecular_weight_per_electron", "flux_scale_jy"):
+        out[f"scaling_{k}"] = np.asarray(getattr(scaling, k))
+    for k in ("r", "theta", "phi", "coeffs"):
+        out[f"brick_{k}"] = np.asarray(getattr(bricks, k))
+    ref_cfg = pr.PolarizedRenderConfig(width=3, height=2, max_steps=40, step=0.18, workers=1)
+    cand_cfg = acc.AcceleratedRenderConfig(width=3, height=2, max_steps=40, step=0.18, progressive_min_width=2)
+    ref = pr.render_stokes_image(ref_cfg, snap, scaling, progress=False)
+    cand = acc.render_stokes_image_bricks(cand_cfg, snap, bricks)
+    m = acc.compare_reference_vs_bricks(ref, cand).metrics
+    out["reg_ref"], out["reg_cand"] = ref, cand
+    out["reg_metrics"] = np.array([m.max_abs, m.mean_abs, m.rmse, m.psnr_db])
+    frames = acc.render_progressive_stokes_bricks(
+        acc.AcceleratedRenderConfig(width=8, height=6, max_steps=30, step=0.2, progressive_min_width=2), snap, bricks)
+    out["prog_levels"] = np.array([[f.level, f.width, f.height] for f in frames])
+    for i, f in enumerate(frames):
+        out[f"prog_{i}"] = f.stokes
+    pt = (float(snap.r[3]), float(snap.theta[3]), float(snap.phi[3]))
+    out["sample_point"] = np.array(pt)
+    out["sample_value"] = acc.sample_coefficient_brick(bricks, *pt)
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/python")
-    ap.add_argument("--only", default="", help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb,accel")
+    ap.add_argument("--only", default="",
+                    help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb,accel,accelreg")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
     from blackhole_sim import accelerated_renderer as acc, benchmark as bench, kerr, native_kernels as nk
-    from blackhole_sim import calibration, grmhd, synchrotron
+    from blackhole_sim import calibration, grmhd, physics, synchrotron
     from blackhole_sim import polarized_transfer as pt
     from blackhole_sim import polarized_renderer as pr
     from blackhole_sim import coefficient_bricks as cb
@@ -495,6 +530,10 @@ def main() -> None:
     if not only or "accel" in only:
         np.savez_compressed(HERE / "accel.npz", **accel_fixtures(cb, acc, kerr, pt, grmhd))
         print("wrote accel.npz")
+    if not only or "accelreg" in only:
+        np.savez_compressed(HERE / "accel_regression.npz",
+                            **accel_regression_fixtures(grmhd, calibration, cb, acc, pr, physics))
+        print("wrote accel_regression.npz")
     if not only or "rgb" in only:
         np.savez_compressed(HERE / "stokes_rgb.npz", **rgb_fixtures(pr))
         print("wrote stokes_rgb.npz")

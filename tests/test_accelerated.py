@@ -216,3 +216,79 @@ def test_gpu_edge_cases(golden):
     assert not np.any(img) and not np.any(diag[..., :3]) and np.all(diag[..., 3] == 0)  # BHN_RAY_MAX_STEPS
     block = acc.render_tile_stokes_bricks(cfg, snap, _golden_bricks(golden), RenderTile(level=0, y0=2, x0=1, x1=4, y1=2))
     assert block.shape == (0, 3, 4)
+
+
+# ---- the reference's own regression test (test_accelerated_renderer.py:17-78) as data
+@pytest.fixture(scope="module")
+def regression():
+    with np.load(Path(__file__).parent / "golden" / "accel_regression.npz") as z:
+        return {k: z[k] for k in z}
+
+
+def _reg_inputs(g):
+    from blackhole_native import grrt
+
+    snap = grrt.Snapshot(**{k: g[f"snap_{k}"] for k in ("r", "theta", "phi", "rho", "theta_e", "pressure", "b_con",
+                                                           "u_con")}, spin_a=float(g["snap_spin_a"]))
+    scaling = grrt.PhysicalScaling(**{k: float(g[f"scaling_{k}"]) for k in (
+        "mass_bh_g", "distance_cm", "rho_cgs_per_code", "b_gauss_per_code", "ion_to_electron_temperature_ratio",
+        "mean_molecular_weight_per_electron", "flux_scale_jy")})
+    return snap, scaling
+
+
+def test_regression_metrics_match_the_reference(regression):
+    """compare_reference_vs_bricks on the reference's own two images gives its metrics."""
+    from blackhole_native import accelerated as acc
+
+    reg = acc.compare_reference_vs_bricks(regression["reg_ref"], regression["reg_cand"])
+    m = reg.metrics
+    assert np.array_equal(np.array([m.max_abs, m.mean_abs, m.rmse, m.psnr_db]), regression["reg_metrics"])
+    assert reg.candidate.shape == reg.reference.shape == (2, 3, 4) and len(m.sha256) == 64
+    with pytest.raises(ValueError, match="shape mismatch"):
+        acc.image_metrics(np.zeros((2, 3, 3)), np.zeros((3, 2, 3)))
+
+
+@pytest.mark.gpu
+def test_gpu_reference_regression_chain(regression, tmp_path):
+    """The reference's small regression end to end on the GPU: the analytic
+    torus snapshot -> precompute_coefficient_bricks -> render_stokes_image_bricks
+    against render_stokes_image, each stage against the reference's own output,
+    and the reference's acceptance bounds (mean_abs <= 0.95, max_abs <= 1)."""
+    from blackhole_native import accelerated as acc
+    from blackhole_native import grrt, synchrotron
+
+    g = regression
+    snap, scaling = _reg_inputs(g)
+    bricks = synchrotron.precompute_coefficient_bricks(snap, scaling, nu_hz=230e9, dtype="float32", stride=1)
+    ref_b = g["brick_coeffs"].astype(np.float64)
+    scale = np.maximum(np.abs(ref_b).max(axis=(0, 1, 2)), 1e-300)
+    assert np.all(np.abs(bricks.coeffs - ref_b) <= 1e-6 * scale)
+    ref = grrt.render_stokes_image(grrt.PolarizedRenderConfig(width=3, height=2, max_steps=40, step=0.18), snap, scaling)
+    for py in range(2):
+        for px in range(3):
+            assert _rel(ref[py, px], g["reg_ref"][py, px]) <= 1e-10, (px, py)
+    cand_cfg = acc.AcceleratedRenderConfig(width=3, height=2, max_steps=40, step=0.18, progressive_min_width=2)
+    cand = acc.render_stokes_image_bricks(cand_cfg, snap, bricks)
+    for py in range(2):
+        for px in range(3):
+            assert _rel(cand[py, px], g["reg_cand"][py, px]) <= TOL, (px, py)
+    reg = acc.compare_reference_vs_bricks(ref, cand)
+    assert np.isfinite(reg.metrics.mean_abs) and reg.metrics.mean_abs <= 0.95 and reg.metrics.max_abs <= 1.0
+    assert np.allclose([reg.metrics.max_abs, reg.metrics.mean_abs], g["reg_metrics"][:2], rtol=0, atol=1e-6)
+
+    frames = acc.render_progressive_stokes_bricks(
+        acc.AcceleratedRenderConfig(width=8, height=6, max_steps=30, step=0.2, progressive_min_width=2), snap, bricks)
+    assert np.array_equal(np.array([[f.level, f.width, f.height] for f in frames]), g["prog_levels"])
+    for i, f in enumerate(frames):
+        want = g[f"prog_{i}"]
+        assert f.stokes.shape == want.shape
+        for idx in np.ndindex(want.shape[:2]):
+            assert _rel(f.stokes[idx], want[idx]) <= TOL if np.any(want[idx]) else not np.any(f.stokes[idx])
+    acc.save_progressive_npz(frames[-1], tmp_path / "f.npz")
+    with np.load(tmp_path / "f.npz") as z:
+        assert z["stokes"].shape == (6, 8, 4)
+
+    grid = SimpleNamespace(r=g["brick_r"], theta=g["brick_theta"], phi=g["brick_phi"], coeffs=g["brick_coeffs"])
+    c = acc.sample_coefficient_brick(grid, *g["sample_point"])
+    assert c is not None and c.shape == (11,) and _rel(c, g["sample_value"]) <= TOL
+    assert acc.sample_coefficient_brick(grid, 1.0e3, 1.0, 1.0) is None
