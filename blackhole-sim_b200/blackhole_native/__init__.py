@@ -19,7 +19,7 @@ import platform as _platform
 import sys as _sys
 
 from . import _lib
-from .bricks import COEFF_NAMES, BrickGrid, torus_brick, horizon_radius
+from .bricks import COEFF_NAMES, BrickGrid, estimate_brick_memory, horizon_radius, torus_brick
 from .kernels import (sample_and_step_stokes, sample_brick_trilinear, sample_brick_valid_mask, stokes_exact_brick,
                       stokes_rk2_brick)
 from .render import (DeviceBrick, PipelinedRenderer, RenderConfig, Renderer, RenderResult, RenderStats, View, render,
@@ -32,7 +32,8 @@ _lib.lib()  # fail loudly at import when the CUDA library is missing
 
 __all__ = [
     "core_version", "detect_arch", "stokes_rk2_brick", "stokes_exact_brick", "sample_brick_trilinear", "sample_and_step_stokes",
-    "sample_brick_valid_mask", "COEFF_NAMES", "BrickGrid", "torus_brick", "horizon_radius", "DeviceBrick",
+    "sample_brick_valid_mask", "COEFF_NAMES", "BrickGrid", "estimate_brick_memory", "torus_brick", "horizon_radius",
+    "DeviceBrick",
     "RenderConfig", "Renderer", "RenderResult", "RenderStats", "View", "render", "render_stokes", "PipelinedRenderer",
     "precompute_coefficient_bricks", "precompute_device_brick", "HybridSynchrotronCoefficients",
     "ThermalSynchrotronCoefficients", "NonthermalPowerLawSynchrotronCoefficients", "accelerated", "grrt", "tiles",

@@ -66,7 +66,7 @@ class BrickGrid:
         expected = (self.r.size, self.theta.size, self.phi.size, len(COEFF_NAMES))
         if c.shape != expected:
             raise ValueError(f"coeffs must have shape {expected}; got {c.shape}")
-        if c.dtype not in (np.float32, np.float64):
+        if c.dtype not in (np.float16, np.float32, np.float64):
             c = c.astype(np.float64)
         object.__setattr__(self, "coeffs", np.ascontiguousarray(c))
 
@@ -120,6 +120,17 @@ class BrickGrid:
                 f.create_dataset(name, data=getattr(self, name), compression="gzip", shuffle=True)
             f.create_dataset("coeffs", data=self.coeffs, compression="gzip", shuffle=True, chunks=True)
             f.create_dataset("coeff_names", data=np.asarray(COEFF_NAMES, dtype="S"))
+
+
+def estimate_brick_memory(nr: int, ntheta: int, nphi: int, dtype: str = "float32") -> dict[str, float]:
+    """coefficient_bricks.py:155-160: bytes of a brick's coefficients and its
+    float32 grids."""
+    bytes_per = np.dtype(dtype).itemsize
+    coeff_bytes = int(nr) * int(ntheta) * int(nphi) * len(COEFF_NAMES) * bytes_per
+    grid_bytes = (int(nr) + int(ntheta) + int(nphi)) * 4
+    total = coeff_bytes + grid_bytes
+    return {"coeff_bytes": float(coeff_bytes), "grid_bytes": float(grid_bytes), "total_bytes": float(total),
+            "total_mib": total / (1024.0 * 1024.0)}
 
 
 def torus_grids(nr: int, ntheta: int, nphi: int, spin_a: float, dtype=np.float32):

@@ -146,7 +146,8 @@ class DeviceBrick:
 
     def __init__(self, brick: BrickGrid, device: torch.device | None = None, precisions: Sequence[str] = ("fp32",)):
         self._init_grids(brick.r, brick.theta, brick.phi, brick.spin_a, device)
-        coeffs = dev.to_device(brick.coeffs.reshape(-1), self.device)
+        c = brick.coeffs.astype(np.float32) if brick.coeffs.dtype == np.float16 else brick.coeffs  # exact widening
+        coeffs = dev.to_device(c.reshape(-1), self.device)
         for p in precisions:
             self._pack(coeffs, p)
 
@@ -207,7 +208,7 @@ class DeviceBrick:
         the non-finite count is read back (one synchronisation).
         """
         src = torch.from_numpy(np.ascontiguousarray(coeffs)) if isinstance(coeffs, np.ndarray) else coeffs
-        src = src.reshape(-1)
+        src = (src.float() if src.dtype == torch.float16 else src).reshape(-1)  # exact widening
         if src.numel() != self.cells * 11:
             raise ValueError(f"coeffs must contain exactly r*theta*phi*11 values; expected {self.cells * 11}, "
                              f"got {src.numel()}")

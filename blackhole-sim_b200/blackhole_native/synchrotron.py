@@ -173,23 +173,34 @@ PIPELINE_SLABS = 8
 
 
 def precompute_coefficient_bricks(snapshot, scaling, nu_hz: float = 230e9,
-                                  dtype: Literal["float32", "float64"] = "float32", coeff_model=None,
+                                  dtype: Literal["float32", "float16", "float64"] = "float32", coeff_model=None,
                                   stride: int = 1) -> BrickGrid:
     """coefficient_bricks.py:119-152 on the GPU; returns the host brick.
 
     Large snapshots go through in r slabs: while the device computes slab k,
     slab k + 1's fields are staged in pinned memory and uploaded on a copy
     stream and slab k - 1's coefficients come back on another, so the
-    transfers hide behind the kernel.  Slabs change no value."""
-    if dtype not in ("float32", "float64"):
-        raise ValueError("dtype must be 'float32' or 'float64'")
+    transfers hide behind the kernel.  Slabs change no value.
+
+    float16 bricks are computed in float64 and cast on the host, each value
+    rounded once as the reference casts its float64 coefficients, then
+    nan_to_num(nan=0, posinf=finfo(float16).max, neginf=0)
+    (coefficient_bricks.py:147-151)."""
+    if dtype not in ("float32", "float16", "float64"):
+        raise ValueError("dtype must be 'float32', 'float16' or 'float64'")
+    work = "float64" if dtype == "float16" else dtype
     r, theta, phi, rho, theta_e, b_con = _fields(snapshot, stride)
     shape = (r.size, theta.size, phi.size)
     if int(np.prod(shape)) < PIPELINE_MIN_CELLS or r.size < 2 * PIPELINE_SLABS:
-        r, theta, phi, out = precompute_device_coefficients(snapshot, scaling, nu_hz, dtype, coeff_model, stride)
-        return BrickGrid(r, theta, phi, out.cpu().numpy(), spin_a=float(snapshot.spin_a))
-    coeffs = _precompute_pipelined(rho, theta_e, b_con, scaling, nu_hz, dtype, coeff_model)
-    return BrickGrid(r, theta, phi, coeffs, spin_a=float(snapshot.spin_a))
+        r, theta, phi, out = precompute_device_coefficients(snapshot, scaling, nu_hz, work, coeff_model, stride)
+        coeffs = out.cpu().numpy()
+    else:
+        coeffs = _precompute_pipelined(rho, theta_e, b_con, scaling, nu_hz, work, coeff_model)
+    if dtype == "float16":
+        with np.errstate(over="ignore"):
+            coeffs = coeffs.astype(np.float16)
+        coeffs = np.nan_to_num(coeffs, nan=0.0, posinf=np.finfo(np.float16).max, neginf=0.0)
+    return BrickGrid(r, theta, phi, coeffs, spin_a=float(snapshot.spin_a), nu_hz=float(nu_hz))
 
 
 def _precompute_pipelined(rho: np.ndarray, theta_e: np.ndarray, b_con: np.ndarray, scaling, nu_hz: float,

@@ -118,7 +118,7 @@ def test_rejects_bad_models(golden):
         bn.precompute_coefficient_bricks(
             snap, scaling, coeff_model=syn.NonthermalPowerLawSynchrotronCoefficients(gamma_min=10.0, gamma_max=5.0))
     with pytest.raises(ValueError, match="dtype"):
-        bn.precompute_coefficient_bricks(snap, scaling, dtype="float16")
+        bn.precompute_coefficient_bricks(snap, scaling, dtype="bfloat16")
 
 
 def test_extreme_plasma_regimes_against_oracle():
@@ -164,3 +164,26 @@ def test_pipelined_host_path_equals_device_path():
         host = bn.precompute_coefficient_bricks(snap, scaling, dtype=dtype)
         dev_out = syn.precompute_device_coefficients(snap, scaling, dtype=dtype)[3].cpu().numpy()
         assert host.coeffs.dtype == dev_out.dtype and np.array_equal(host.coeffs, dev_out)
+
+
+def test_precompute_float16_and_stride(golden):
+    """dtype="float16" (test_coefficient_bricks.py:30-35, coefficient_bricks.py:
+    140-151): the float64 coefficients rounded once to float16, then
+    nan_to_num(nan=0, posinf=finfo(float16).max, neginf=0); a float16 brick
+    widens exactly to the renderer's float32 records."""
+    g, snap, scaling = golden
+    b = bn.precompute_coefficient_bricks(snap, scaling, nu_hz=230e9, dtype="float16", stride=2)
+    ref64 = g["coeffs64_230_stride2"]
+    with np.errstate(over="ignore"):
+        want = np.nan_to_num(ref64.astype(np.float16), nan=0.0, posinf=np.finfo(np.float16).max, neginf=0.0)
+    assert b.coeffs.dtype == np.float16 and b.coeffs.shape == want.shape and b.nu_hz == 230e9
+    assert np.array_equal(b.coeffs, want)
+    scaled = bn.BrickGrid(b.r, b.theta, b.phi, (ref64 * (1.0 / max(np.abs(ref64).max(), 1e-300))).astype(np.float16),
+                          spin_a=b.spin_a)
+    view = bn.View(24, 24, spin_a=b.spin_a, r_obs=30.0, inclination_deg=70.0, fov_y_deg=30.0, max_steps=900)
+    img16 = bn.render(bn.DeviceBrick(scaled), view).image().cpu().numpy()
+    wide = bn.BrickGrid(b.r, b.theta, b.phi, scaled.coeffs.astype(np.float32), spin_a=b.spin_a)
+    img32 = bn.render(bn.DeviceBrick(wide), view).image().cpu().numpy()
+    assert np.array_equal(img16, img32)
+    with pytest.raises(ValueError, match="dtype"):
+        bn.precompute_coefficient_bricks(snap, scaling, dtype="int8")

@@ -119,3 +119,19 @@ def test_render_prepare_rejects_outputs_beyond_32_bit_indices():
     aligned = (ctypes.addressof(scratch) + 255) & ~255
     rc = L.bhn_render_prepare(ctypes.byref(v), 1, aligned, 1 << 16, None)
     assert rc == 1 and b"2^32" in L.bhn_last_error()
+
+
+def test_estimate_brick_memory_and_float16_bricks(tmp_path):
+    """coefficient_bricks.py:155-160 and float16 CoefficientBrickGrid values
+    (kept as float16, through the npz round trip)."""
+    est = bn.estimate_brick_memory(8, 6, 4, "float32")
+    assert est["coeff_bytes"] == 8 * 6 * 4 * 11 * 4 and est["grid_bytes"] == 18 * 4
+    assert est["total_bytes"] == est["coeff_bytes"] + est["grid_bytes"] > 8 * 6 * 4 * 11 * 3
+    assert est["total_mib"] == est["total_bytes"] / (1024.0 * 1024.0)
+    assert bn.estimate_brick_memory(8, 6, 4, "float16")["coeff_bytes"] == 8 * 6 * 4 * 11 * 2
+    b = bricks.torus_brick(5, 4, 3, spin_a=0.5, seed=2, dtype=np.float32)
+    h = bn.BrickGrid(b.r, b.theta, b.phi, b.coeffs.astype(np.float16), spin_a=0.5, nu_hz=86e9)
+    assert h.coeffs.dtype == np.float16
+    h.save_npz(tmp_path / "h.npz")
+    back = bn.BrickGrid.load_npz(tmp_path / "h.npz")
+    assert back.coeffs.dtype == np.float16 and np.array_equal(back.coeffs, h.coeffs) and back.nu_hz == 86e9
