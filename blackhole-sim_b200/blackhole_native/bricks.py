@@ -78,6 +78,17 @@ class BrickGrid:
     def cells(self) -> int:
         return int(self.r.size * self.theta.size * self.phi.size)
 
+    @property
+    def dtype_name(self) -> str:
+        """coefficient_bricks.py:35: the coefficients' dtype name."""
+        return self.coeffs.dtype.name
+
+    @property
+    def bytes(self) -> int:
+        """coefficient_bricks.py:51-53: coefficient bytes plus the grids as the
+        reference stores them (float32)."""
+        return int(self.coeffs.nbytes + 4 * (self.r.size + self.theta.size + self.phi.size))
+
     def save_npz(self, path) -> None:
         """The file layout of CoefficientBrickGrid.save_npz (coefficient_bricks.py:57-70):
         r, theta, phi, coeffs, coeff_names, nu_hz, spin_a, dtype_name; the

@@ -135,3 +135,10 @@ def test_estimate_brick_memory_and_float16_bricks(tmp_path):
     h.save_npz(tmp_path / "h.npz")
     back = bn.BrickGrid.load_npz(tmp_path / "h.npz")
     assert back.coeffs.dtype == np.float16 and np.array_equal(back.coeffs, h.coeffs) and back.nu_hz == 86e9
+
+
+def test_brick_grid_reports_dtype_and_bytes():
+    b = bricks.torus_brick(5, 4, 3, spin_a=0.5, seed=2, dtype=np.float32)
+    assert b.dtype_name == "float32" and b.bytes == b.coeffs.nbytes + 4 * (5 + 4 + 3)
+    est = bn.estimate_brick_memory(5, 4, 3, "float32")
+    assert b.bytes == est["total_bytes"]
