@@ -19,7 +19,9 @@ and grrt (the physical polarized renderer's default 160 x 90 image, pixels/s),
 whose lines carry an FP64 exp() roofline measured in the same run; learned
 (time to an image at 1e-3 Stokes-I error: the learned step size against plain
 RK2 and the step-doubling controller); bricks (the reference's own fixed-step
-RK4 brick renderer, its default 160 x 90 image, pixels/s, FP64 roofline).
+RK4 brick renderer, its default 160 x 90 image, pixels/s, FP64 roofline);
+micro (the plugin's sample_and_step_stokes on 16.8M points, points/s, HBM
+roofline).
 For N > 1 the job runs as torchrun ranks, one full image per rank (replicas:
 rays are independent and the path has no exchange step).
 """
@@ -948,6 +950,134 @@ def bricks_cpu_baseline(grid, snap, cfg, target_s: float) -> dict:
                       f"({segs} sampled segments) in {dt:.2f} s"}
 
 
+# The plugin's sample_and_step_stokes (native_kernels.py:325-407, lib.rs:308-366)
+MICRO = dict(nr=256, ntheta=128, nphi=256, points=1 << 24, seed=0, ds_cm=0.05, e2e_points=1 << 20)
+MICRO_PROFILE = REPO / "profiles" / "sample_and_step_kernel_16M_points.md"
+# Algorithmic bytes per point: the (r, theta, phi) triple, the 8 corner cells'
+# 11 float64 coefficients, the 4 float64 Stokes values written (the initial
+# vector is broadcast).
+MICRO_BYTES_PER_POINT = 3 * 8 + 8 * 11 * 8 + 4 * 8
+
+
+def bench_micro(args) -> dict | None:
+    """The plugin micro-kernel sample_and_step_stokes at scale: one step =
+    16.8M seeded points inside a 256 x 128 x 256 x 11 float64 torus brick
+    (738 MB, larger than L2), each sampled trilinearly and advanced by one
+    Stokes RK2 step, FP64, on device tensors; e2e through the reference-facing
+    call (host arrays in, the brick passed every call, a flat list out)."""
+    import torch
+
+    from blackhole_native import _device as dev
+    from blackhole_native import _lib, bricks, kernels
+
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    init_dist(world, "nccl")
+    stream = torch.cuda.current_stream(device)
+    M = MICRO
+    b = bricks.torus_brick(M["nr"], M["ntheta"], M["nphi"], spin_a=0.9375, seed=M["seed"], dtype=np.float64)
+    n = int(args.side) * 1024 if args.side else M["points"]
+    rng = np.random.default_rng(M["seed"] + 1)
+    pts = np.empty((n, 3))
+    pts[:, 0] = rng.uniform(b.r[0], b.r[-1], n)
+    pts[:, 1] = rng.uniform(b.theta[0], b.theta[-1], n)
+    pts[:, 2] = rng.uniform(0.0, 2.0 * math.pi, n)
+    c = torch.as_tensor(b.coeffs.reshape(-1), device=device)
+    rg, tg, pg = (torch.as_tensor(g, device=device) for g in (b.r, b.theta, b.phi))
+    dp = torch.as_tensor(pts, device=device)
+    ini = torch.zeros(4, dtype=torch.float64, device=device)
+    ref = kernels.sample_and_step_stokes(c, rg, tg, pg, dp, M["ds_cm"], ini)  # the checked public tensor call
+    out = torch.empty_like(ref)
+    L = _lib.lib()
+
+    def launch():  # the same kernel through the C ABI, without the per-call input checks
+        _lib.check(L.bhn_sample_and_step_stokes(dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(),
+                                                dev.ptr(pg), pg.numel(), dev.ptr(dp), n, M["ds_cm"], dev.ptr(ini), 4,
+                                                0, dev.ptr(out), stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        launch()
+    clocks = ClockSampler(_uuid(device)).start()
+    time.sleep(0.3)
+    barrier(world)
+    per = timed_launches(launch, args.steps, stream, device)
+    barrier(world)
+    clk = clocks.stop()
+    assert torch.equal(out, ref), "outputs differ between launches"
+    t_max = max_over_ranks(sum(per), world, device)
+    value = sum_over_ranks(n * args.steps, world, device) / (t_max * 1e-3)
+
+    e2e = None
+    if not args.no_e2e:  # host numpy in, flat list out, the brick passed with every call (the reference's call)
+        ne = min(n, M["e2e_points"])
+        host = [b.coeffs.reshape(-1), b.r, b.theta, b.phi, pts[:ne]]
+        ke = max(1, min(args.steps, 3))
+        barrier(world)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        a0.record(stream)
+        for _ in range(ke):
+            lst = kernels.sample_and_step_stokes(*host, M["ds_cm"], [0.0, 0.0, 0.0, 0.0])
+        a1.record(stream)
+        torch.cuda.synchronize(device)
+        barrier(world)
+        te = max_over_ranks(a0.elapsed_time(a1), world, device)
+        assert np.array_equal(np.asarray(lst), ref[: 4 * ne].cpu().numpy()), "list API differs from the tensor call"
+        e2e = {"value": sum_over_ranks(ne * ke, world, device) / (te * 1e-3), "unit": "points/s",
+               "h2d_bytes_per_step": int(sum(x.nbytes for x in host) + 32), "d2h_bytes_per_step": int(ne * 32),
+               "ms_per_step": te / ke, "api": "sample_and_step_stokes (numpy in, list out)",
+               "points_per_step": ne}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = micro_cpu_baseline(b, pts, M["ds_cm"], args.cpu_seconds)
+    per_mean = statistics.mean(per)
+    peaks = load_peaks()
+    achieved = MICRO_BYTES_PER_POINT * n / (per_mean * 1e-3) / 1e9
+    line = {
+        "metric": "points/s", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"plugin sample_and_step_stokes: {n} seeded points inside a {M['nr']}x{M['ntheta']}x"
+                               f"{M['nphi']}x11 float64 torus brick, ds_cm {M['ds_cm']}, broadcast initial",
+                   "points_per_step": n, "l2": "brick (738 MB) larger than L2; points uniform over the domain",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "e2e": e2e, "gpu_launches": args.steps, "clocks": clk,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": profiled_traffic(MICRO_PROFILE),
+                     "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)" if peaks["source"] == "measured"
+                     else "fallback 6.65 TB/s",
+                     "kernel": "sample_and_step_kernel", "algorithmic_bytes_per_point": MICRO_BYTES_PER_POINT},
+        "cpu_baseline": cpu,
+        "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
+    }
+    if world > 1:
+        import torch.distributed as td
+
+        td.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def micro_cpu_baseline(b, pts, ds_cm: float, target_s: float) -> dict:
+    """The float64 oracle (oracle/bhoracle.c bho_sample_and_step_stokes, one core) on a prefix of the points."""
+    sys.path.insert(0, str(REPO))
+    from oracle import oracle as O
+
+    coeffs = b.coeffs.reshape(-1)
+    n = 1 << 16
+    t0 = time.perf_counter()
+    O.sample_and_step_stokes(coeffs, b.r, b.theta, b.phi, pts[:n], ds_cm, np.zeros(4))
+    dt = time.perf_counter() - t0
+    if dt < target_s / 4:
+        n = min(len(pts), int(n * target_s / max(dt, 1e-3)))
+        t0 = time.perf_counter()
+        O.sample_and_step_stokes(coeffs, b.r, b.theta, b.phi, pts[:n], ds_cm, np.zeros(4))
+        dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "points/s", "cores": 1, "kind": "port",
+            "sample": f"float64 oracle (oracle/bhoracle.c, one core): {n} of the points in {dt:.2f} s"}
+
+
 def _scaled_traffic(summary: Path, scale: float) -> float | None:
     t = profiled_traffic(summary)
     return None if t is None else t * scale
@@ -1078,16 +1208,17 @@ def main(argv=None) -> int:
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="target length of one reference-arm step")
     ap.add_argument("--config", type=json.loads, default=None, help="RenderConfig fields as JSON (skips autotune)")
     ap.add_argument("--tune", action="store_true", help="run the launch-shape autotuner on the workload and exit")
-    ap.add_argument("--workload", choices=["image", "views", "precompute", "grrt", "learned", "bricks"],
+    ap.add_argument("--workload", choices=["image", "views", "precompute", "grrt", "learned", "bricks", "micro"],
                     default="image",
                     help="image: the 1024x1024 single view (default); views: many uneven views in one launch; "
                          "precompute: coefficient bricks from a snapshot; grrt: the physical polarized renderer; "
                          "learned: time to an image at 1e-3, learned step size against plain RK2; bricks: the "
-                         "reference's own brick renderer (fixed-step RK4)")
+                         "reference's own brick renderer (fixed-step RK4); micro: the plugin's "
+                         "sample_and_step_stokes at 16.8M points")
     ap.add_argument("--n-views", type=int, default=256)
     ap.add_argument("--side", type=int, default=0,
                     help="profiling only: image workload side x side rays; precompute nr = side; grrt and "
-                         "bricks image side x side*9/16")
+                         "bricks image side x side*9/16; micro side*1024 points")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps, whatever is asked
     if args.impl == "reference":
@@ -1102,6 +1233,8 @@ def main(argv=None) -> int:
         line = bench_learned(args)
     elif args.workload == "bricks":
         line = bench_bricks(args)
+    elif args.workload == "micro":
+        line = bench_micro(args)
     else:
         line = bench_ours(args)
     if line is not None:
