@@ -198,9 +198,7 @@ def sample_and_step_stokes(coeffs, r_grid, theta_grid, phi_grid, points, ds_cm, 
         if dev.check_values_device(ini, False)[0]:
             raise ValueError("initial must contain only finite values")
         out = torch.empty(n * STOKES_COMPONENTS, dtype=torch.float64, device=device)
-        _lib.check(_lib.lib().bhn_sample_and_step_stokes(dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(),
-                                                         dev.ptr(pg), pg.numel(), dev.ptr(pts), n, ds, dev.ptr(ini),
-                                                         ini.numel(), policy, dev.ptr(out), dev.stream_ptr()))
+        _launch_sample_and_step(c, rg, tg, pg, pts, n, ds, ini, policy, out)
         return out
     c, rg, tg, pg, pts = (dev.host_f64(x) for x in (coeffs, r_grid, theta_grid, phi_grid, points))
     n = _validate_sampler_host(c, rg, tg, pg, pts)
@@ -212,10 +210,28 @@ def sample_and_step_stokes(coeffs, r_grid, theta_grid, phi_grid, points, ds_cm, 
     device = dev.require_cuda()
     d = [dev.to_device(x, device) for x in (c, rg, tg, pg, pts, ini)]
     out = torch.empty(n * STOKES_COMPONENTS, dtype=torch.float64, device=device)
-    _lib.check(_lib.lib().bhn_sample_and_step_stokes(dev.ptr(d[0]), dev.ptr(d[1]), rg.size, dev.ptr(d[2]), tg.size,
-                                                     dev.ptr(d[3]), pg.size, dev.ptr(d[4]), n, ds, dev.ptr(d[5]),
-                                                     ini.size, policy, dev.ptr(out), dev.stream_ptr()))
+    _launch_sample_and_step(*d[:5], n, ds, d[5], policy, out)
     return out.cpu().numpy().tolist()
+
+
+SORT_MIN_POINTS = 1 << 18   # from this many points the sampler takes them in brick-cell order
+
+
+def _launch_sample_and_step(c, rg, tg, pg, pts, n: int, ds: float, ini, policy: int, out) -> None:
+    """bhn_sample_and_step_stokes, or for large point sets its cell-ordered form
+    (bhn_sample_and_step_stokes_sorted: the same values, neighbouring points
+    sharing cached corners); every argument already on the device."""
+    L = _lib.lib()
+    args = (dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(), dev.ptr(pg), pg.numel(), dev.ptr(pts), n, ds,
+            dev.ptr(ini), ini.numel(), policy, dev.ptr(out))
+    nbytes = int(L.bhn_sample_sort_scratch_bytes(n, rg.numel() * tg.numel() * pg.numel())) if n >= SORT_MIN_POINTS \
+        else -1
+    if nbytes <= 0:
+        _lib.check(L.bhn_sample_and_step_stokes(*args, dev.stream_ptr()))
+        return
+    scratch = torch.empty(nbytes + 256, dtype=torch.uint8, device=out.device)
+    sp = (dev.ptr(scratch) + 255) & ~255
+    _lib.check(L.bhn_sample_and_step_stokes_sorted(*args, sp, nbytes, dev.stream_ptr()))
 
 
 def sample_brick_valid_mask(r_grid, theta_grid, points):

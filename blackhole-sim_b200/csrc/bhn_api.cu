@@ -16,6 +16,8 @@
 #include "bhn_transfer.cuh"
 #include "bhn_exact.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
+
 namespace bhn {
 
 static thread_local std::string g_last_error;
@@ -93,21 +95,65 @@ __global__ void sample_and_step_kernel(const double *__restrict__ coeffs, const 
                                        const double *__restrict__ tg, int nt, const double *__restrict__ pg, int np,
                                        const double *__restrict__ pts, int64_t n, double ds,
                                        const double *__restrict__ initial, int broadcast, int policy,
-                                       double *__restrict__ out) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double c[11];
-        const double *s0 = initial + (broadcast ? 0 : 4 * i);
-        double s[4] = {s0[0], s0[1], s0[2], s0[3]};
-        if (sample_one_exact(coeffs, rg, nr, tg, nt, pg, np, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], c)) {
-            stokes_step_rk2_exact(s, c, ds);
-        } else if (policy == BHN_POLICY_ZERO) {
-            s[0] = s[1] = s[2] = s[3] = 0.0;
-        } else if (policy != BHN_POLICY_INITIAL) {
-            s[0] = s[1] = s[2] = s[3] = __longlong_as_double(0x7ff8000000000000ULL);
-        }
-        reinterpret_cast<double2 *>(out + 4 * i)[0] = make_double2(s[0], s[1]);
-        reinterpret_cast<double2 *>(out + 4 * i)[1] = make_double2(s[2], s[3]);
+                                       double *__restrict__ out);
+
+// One Stokes RK2 sample-and-step of point i (native_kernels.py:325-407 with the policy of :391-397).
+__device__ __forceinline__ void sample_and_step_point(const double *__restrict__ coeffs, const double *__restrict__ rg,
+                                                      int nr, const double *__restrict__ tg, int nt,
+                                                      const double *__restrict__ pg, int np,
+                                                      const double *__restrict__ pts, int64_t i, double ds,
+                                                      const double *__restrict__ initial, int broadcast, int policy,
+                                                      double *__restrict__ out) {
+    double c[11];
+    const double *s0 = initial + (broadcast ? 0 : 4 * i);
+    double s[4] = {s0[0], s0[1], s0[2], s0[3]};
+    if (sample_one_exact(coeffs, rg, nr, tg, nt, pg, np, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], c)) {
+        stokes_step_rk2_exact(s, c, ds);
+    } else if (policy == BHN_POLICY_ZERO) {
+        s[0] = s[1] = s[2] = s[3] = 0.0;
+    } else if (policy != BHN_POLICY_INITIAL) {
+        s[0] = s[1] = s[2] = s[3] = __longlong_as_double(0x7ff8000000000000ULL);
     }
+    reinterpret_cast<double2 *>(out + 4 * i)[0] = make_double2(s[0], s[1]);
+    reinterpret_cast<double2 *>(out + 4 * i)[1] = make_double2(s[2], s[3]);
+}
+
+// The cell (r0, theta0, phi0) a point samples from, as one index; points the
+// sampler rejects (outside the nonperiodic r/theta range, non-finite) sort last.
+__global__ void cell_key_kernel(const double *__restrict__ rg, int nr, const double *__restrict__ tg, int nt,
+                                const double *__restrict__ pg, int np, const double *__restrict__ pts, int64_t n,
+                                uint32_t invalid_key, uint32_t *__restrict__ keys, uint32_t *__restrict__ idx) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int r0, t0, p0, p1;
+        double wr, wt, wp;
+        uint32_t key = invalid_key;
+        if (bracket_linear_exact(rg, nr, pts[3 * i], r0, wr) && bracket_linear_exact(tg, nt, pts[3 * i + 1], t0, wt)) {
+            bracket_phi_exact(pg, np, pts[3 * i + 2], p0, p1, wp);
+            key = (uint32_t)(((int64_t)r0 * nt + t0) * np + p0);
+        }
+        keys[i] = key;
+        idx[i] = (uint32_t)i;
+    }
+}
+
+__global__ void sample_and_step_kernel(const double *__restrict__ coeffs, const double *__restrict__ rg, int nr,
+                                       const double *__restrict__ tg, int nt, const double *__restrict__ pg, int np,
+                                       const double *__restrict__ pts, int64_t n, double ds,
+                                       const double *__restrict__ initial, int broadcast, int policy,
+                                       double *__restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        sample_and_step_point(coeffs, rg, nr, tg, nt, pg, np, pts, i, ds, initial, broadcast, policy, out);
+}
+
+__global__ void sample_and_step_ordered_kernel(const double *__restrict__ coeffs, const double *__restrict__ rg,
+                                               int nr, const double *__restrict__ tg, int nt,
+                                               const double *__restrict__ pg, int np, const double *__restrict__ pts,
+                                               const uint32_t *__restrict__ order, int64_t n, double ds,
+                                               const double *__restrict__ initial, int broadcast, int policy,
+                                               double *__restrict__ out) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        sample_and_step_point(coeffs, rg, nr, tg, nt, pg, np, pts, (int64_t)order[k], ds, initial, broadcast, policy,
+                              out);
 }
 
 __global__ void valid_mask_kernel(const double *__restrict__ rg, int nr, const double *__restrict__ tg, int nt,
@@ -382,6 +428,82 @@ int bhn_sample_and_step_stokes(const double *coeffs, const double *r_grid, int64
         coeffs, r_grid, (int)nr, theta_grid, (int)nt, phi_grid, (int)np, points, n_points, ds_cm, initial,
         initial_len == 4, invalid_policy, out);
     BHN_LAUNCH_CHECK("sample_and_step_kernel");
+    return BHN_OK;
+}
+
+namespace {
+struct SortLayout {
+    int64_t keys_in, keys_out, idx_in, idx_out, temp, temp_bytes, total;
+};
+
+int key_bits(uint32_t max_key) {
+    int b = 1;
+    while (b < 32 && (max_key >> b)) ++b;
+    return b;
+}
+
+// Offsets of the key / index arrays and the radix sort's temporary storage in
+// the caller's scratch (each 256-byte aligned).  total < 0: unsupported sizes.
+SortLayout sort_layout(int64_t n, int64_t cells) {
+    SortLayout L{};
+    L.total = -1;
+    if (n <= 0 || n > INT32_MAX || cells <= 0 || cells >= (int64_t)UINT32_MAX) return L;
+    size_t temp = 0;
+    if (cub::DeviceRadixSort::SortPairs(nullptr, temp, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                        (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n, 0,
+                                        key_bits((uint32_t)cells)) != cudaSuccess)
+        return L;
+    auto up = [](int64_t x) { return (x + 255) & ~(int64_t)255; };
+    const int64_t a = up(4 * n);
+    L.keys_in = 0;
+    L.keys_out = a;
+    L.idx_in = 2 * a;
+    L.idx_out = 3 * a;
+    L.temp = 4 * a;
+    L.temp_bytes = (int64_t)temp;
+    L.total = 4 * a + up((int64_t)temp);
+    return L;
+}
+}  // namespace
+
+int64_t bhn_sample_sort_scratch_bytes(int64_t n_points, int64_t cells) { return sort_layout(n_points, cells).total; }
+
+int bhn_sample_and_step_stokes_sorted(const double *coeffs, const double *r_grid, int64_t nr,
+                                      const double *theta_grid, int64_t nt, const double *phi_grid, int64_t np,
+                                      const double *points, int64_t n_points, double ds_cm, const double *initial,
+                                      int64_t initial_len, int32_t invalid_policy, double *out, void *scratch,
+                                      int64_t scratch_bytes, void *stream) {
+    if (!std::isfinite(ds_cm) || ds_cm < 0.0) return fail(BHN_ERR_VALUE, "ds_cm must be finite and non-negative");
+    int rc = check_grid_sizes(nr, nt, np);
+    if (rc) return rc;
+    if (invalid_policy < 0 || invalid_policy > 2)
+        return fail(BHN_ERR_VALUE, "invalid_policy must be 'nan', 'initial', or 'zero'");
+    if (n_points < 0) return fail(BHN_ERR_VALUE, "points must contain flat r, theta, phi triples");
+    if (initial_len != 4 && initial_len != 4 * n_points)
+        return fail(BHN_ERR_VALUE, "initial must contain either 4 values or 4 values per sample point");
+    if (n_points == 0) return BHN_OK;
+    const int64_t cells = nr * nt * np;
+    const SortLayout L = sort_layout(n_points, cells);
+    if (L.total < 0) return fail(BHN_ERR_VALUE, "point count or brick size outside the sorted path's range");
+    if (!scratch || scratch_bytes < L.total || (reinterpret_cast<uintptr_t>(scratch) & 255))
+        return fail(BHN_ERR_VALUE, "scratch must be 256-byte aligned and hold bhn_sample_sort_scratch_bytes bytes");
+    unsigned char *base = static_cast<unsigned char *>(scratch);
+    uint32_t *keys_in = reinterpret_cast<uint32_t *>(base + L.keys_in);
+    uint32_t *keys_out = reinterpret_cast<uint32_t *>(base + L.keys_out);
+    uint32_t *idx_in = reinterpret_cast<uint32_t *>(base + L.idx_in);
+    uint32_t *idx_out = reinterpret_cast<uint32_t *>(base + L.idx_out);
+    cudaStream_t s = as_stream(stream);
+    cell_key_kernel<<<grid_for(n_points, 256), 256, 0, s>>>(r_grid, (int)nr, theta_grid, (int)nt, phi_grid, (int)np,
+                                                          points, n_points, (uint32_t)cells, keys_in, idx_in);
+    BHN_LAUNCH_CHECK("cell_key_kernel");
+    size_t temp = (size_t)L.temp_bytes;
+    if (cub::DeviceRadixSort::SortPairs(base + L.temp, temp, keys_in, keys_out, idx_in, idx_out, (int)n_points, 0,
+                                        key_bits((uint32_t)cells), s) != cudaSuccess)
+        return fail(BHN_ERR_CUDA, "radix sort of the point cells failed");
+    sample_and_step_ordered_kernel<<<grid_for(n_points, 128), 128, 0, s>>>(
+        coeffs, r_grid, (int)nr, theta_grid, (int)nt, phi_grid, (int)np, points, idx_out, n_points, ds_cm, initial,
+        initial_len == 4, invalid_policy, out);
+    BHN_LAUNCH_CHECK("sample_and_step_ordered_kernel");
     return BHN_OK;
 }
 

@@ -102,6 +102,21 @@ int bhn_sample_and_step_stokes(const double *coeffs, const double *r_grid, int64
                                int64_t n_points, double ds_cm, const double *initial, int64_t initial_len,
                                int32_t invalid_policy, double *out, void *stream);
 
+/* bhn_sample_and_step_stokes with the points taken in brick-cell order: a
+ * key kernel brackets every point (cell index, or past-the-end for points
+ * outside the nonperiodic r/theta domain), a radix sort orders the point
+ * indices by cell, and the sampler walks that order, writing each result to
+ * its point's own row -- the same values, bit for bit, with neighbouring
+ * points sharing cached corners.  For 0 < n_points < 2^31 and cells < 2^32 - 1;
+ * scratch: bhn_sample_sort_scratch_bytes(n_points, nr * nt * np) bytes,
+ * 256-byte aligned, on the device. */
+int64_t bhn_sample_sort_scratch_bytes(int64_t n_points, int64_t cells);
+int bhn_sample_and_step_stokes_sorted(const double *coeffs, const double *r_grid, int64_t nr,
+                                      const double *theta_grid, int64_t nt, const double *phi_grid, int64_t np,
+                                      const double *points, int64_t n_points, double ds_cm, const double *initial,
+                                      int64_t initial_len, int32_t invalid_policy, double *out, void *scratch,
+                                      int64_t scratch_bytes, void *stream);
+
 /* Replaces sample_brick_valid_mask (native_kernels.py:189-210, Python-only in
  * the reference): inclusive r/theta bounds, phi ignored.  mask: n bytes (0/1). */
 int bhn_sample_brick_valid_mask(const double *r_grid, int64_t nr, const double *theta_grid, int64_t nt,

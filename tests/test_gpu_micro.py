@@ -157,3 +157,46 @@ def test_throughput_probes_run_and_count():
     torch.cuda.synchronize()
     assert L.bhn_fp64_peak_probe(scratch.data_ptr(), 2, 1, 2, ctypes.byref(ops), None) != 0
     assert b"probe mode" in L.bhn_last_error()
+
+
+def test_cell_ordered_sampler_equals_the_plain_kernel():
+    """bhn_sample_and_step_stokes_sorted (points taken in brick-cell order,
+    results written to their own rows) gives the plain kernel's bits for every
+    policy, broadcast and per-point initial vectors, points outside the domain,
+    on knots and NaN points."""
+    import torch
+
+    from blackhole_native import _device as dev
+    from blackhole_native import _lib, bricks, kernels
+
+    b = bricks.torus_brick(24, 16, 20, spin_a=0.9, seed=3, dtype=np.float64)
+    rng = np.random.default_rng(5)
+    n = kernels.SORT_MIN_POINTS + 12345
+    lo = [b.r[0] - 1.0, b.theta[0] - 0.1, -7.0]
+    hi = [b.r[-1] + 1.0, b.theta[-1] + 0.1, 7.0]
+    pts = rng.uniform(lo, hi, (n, 3))
+    pts[::997] = np.nan
+    pts[1::991, 0] = b.r[-1]
+    pts[2::983, 1] = b.theta[0]
+    pts[3::977, 2] = b.phi[0] + 2.0 * np.pi
+    device = torch.device("cuda", 0)
+    c = torch.as_tensor(b.coeffs.reshape(-1), device=device)
+    rg, tg, pg = (torch.as_tensor(g, device=device) for g in (b.r, b.theta, b.phi))
+    dp = torch.as_tensor(pts, device=device)
+    L = _lib.lib()
+    for per_point in (False, True):
+        ini = torch.as_tensor(rng.normal(0.0, 1.0, 4 * n if per_point else 4), device=device)
+        for policy in (0, 1, 2):
+            plain = torch.empty(4 * n, dtype=torch.float64, device=device)
+            _lib.check(L.bhn_sample_and_step_stokes(dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(),
+                                                    dev.ptr(pg), pg.numel(), dev.ptr(dp), n, 0.07, dev.ptr(ini),
+                                                    ini.numel(), policy, dev.ptr(plain), dev.stream_ptr()))
+            ordered = torch.empty_like(plain)
+            kernels._launch_sample_and_step(c, rg, tg, pg, dp, n, 0.07, ini, policy, ordered)
+            assert torch.equal(plain.view(torch.int64), ordered.view(torch.int64)), (per_point, policy)
+    assert L.bhn_sample_sort_scratch_bytes(n, b.cells) > 16 * n
+    assert L.bhn_sample_sort_scratch_bytes(0, b.cells) == -1 and L.bhn_sample_sort_scratch_bytes(n, 0) == -1
+    rc = L.bhn_sample_and_step_stokes_sorted(dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(),
+                                             dev.ptr(pg), pg.numel(), dev.ptr(dp), n, 0.07, dev.ptr(ini), ini.numel(),
+                                             0, dev.ptr(plain), None, 0, dev.stream_ptr())
+    assert rc == 1 and b"scratch" in L.bhn_last_error()
