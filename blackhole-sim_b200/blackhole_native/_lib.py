@@ -20,7 +20,7 @@ RAY_STATUS = ("max_steps", "captured", "escaped", "invalid", "optically_thick")
 EXPORTED = (
     "bhn_core_version", "bhn_last_error", "bhn_device_info", "bhn_fp32_peak_probe", "bhn_fp64_peak_probe",
     "bhn_stokes_rk2_brick", "bhn_stokes_exact_brick", "bhn_sample_brick_trilinear", "bhn_sample_and_step_stokes",
-    "bhn_sample_sort_scratch_bytes", "bhn_sample_and_step_stokes_sorted",
+    "bhn_sample_sort_scratch_bytes", "bhn_sample_and_step_stokes_sorted", "bhn_sample_brick_trilinear_sorted",
     "bhn_sample_brick_valid_mask", "bhn_check_values",
     "bhn_brick_tables_bytes", "bhn_brick_build_tables", "bhn_brick_pack", "bhn_brick_locate",
     "bhn_render_scratch_bytes", "bhn_render_prepare", "bhn_render_launch", "bhn_render_noalloc",
@@ -118,6 +118,7 @@ def _declare(lib: ctypes.CDLL) -> None:
         "bhn_sample_and_step_stokes": ([vp, vp, i64, vp, i64, vp, i64, vp, i64, d, vp, i64, i32, vp, vp],
                                        ctypes.c_int),
         "bhn_sample_sort_scratch_bytes": ([i64, i64], ctypes.c_int64),
+        "bhn_sample_brick_trilinear_sorted": ([vp, vp, i64, vp, i64, vp, i64, vp, i64, vp, vp, i64, vp], ctypes.c_int),
         "bhn_sample_and_step_stokes_sorted": ([vp, vp, i64, vp, i64, vp, i64, vp, i64, d, vp, i64, i32, vp, vp, i64,
                                                vp], ctypes.c_int),
         "bhn_sample_brick_valid_mask": ([vp, i64, vp, i64, vp, i64, vp, vp], ctypes.c_int),

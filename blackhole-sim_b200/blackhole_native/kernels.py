@@ -161,18 +161,14 @@ def sample_brick_trilinear(coeffs, r_grid, theta_grid, phi_grid, points):
         c, rg, tg, pg, pts = (_dev_f64(torch.as_tensor(x), device) for x in (coeffs, r_grid, theta_grid, phi_grid, points))
         n = _validate_sampler_device(c, rg, tg, pg, pts)
         out = torch.empty(n * COEFFS_PER_CELL, dtype=torch.float64, device=device)
-        _lib.check(_lib.lib().bhn_sample_brick_trilinear(dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(),
-                                                         dev.ptr(pg), pg.numel(), dev.ptr(pts), n, dev.ptr(out),
-                                                         dev.stream_ptr()))
+        _launch_sample_trilinear(c, rg, tg, pg, pts, n, out)
         return out
     c, rg, tg, pg, pts = (dev.host_f64(x) for x in (coeffs, r_grid, theta_grid, phi_grid, points))
     n = _validate_sampler_host(c, rg, tg, pg, pts)
     device = dev.require_cuda()
     d = [dev.to_device(x, device) for x in (c, rg, tg, pg, pts)]
     out = torch.empty(n * COEFFS_PER_CELL, dtype=torch.float64, device=device)
-    _lib.check(_lib.lib().bhn_sample_brick_trilinear(dev.ptr(d[0]), dev.ptr(d[1]), rg.size, dev.ptr(d[2]), tg.size,
-                                                     dev.ptr(d[3]), pg.size, dev.ptr(d[4]), n, dev.ptr(out),
-                                                     dev.stream_ptr()))
+    _launch_sample_trilinear(*d, n, out)
     return out.cpu().numpy().tolist()
 
 
@@ -232,6 +228,21 @@ def _launch_sample_and_step(c, rg, tg, pg, pts, n: int, ds: float, ini, policy: 
     scratch = torch.empty(nbytes + 256, dtype=torch.uint8, device=out.device)
     sp = (dev.ptr(scratch) + 255) & ~255
     _lib.check(L.bhn_sample_and_step_stokes_sorted(*args, sp, nbytes, dev.stream_ptr()))
+
+
+def _launch_sample_trilinear(c, rg, tg, pg, pts, n: int, out) -> None:
+    """bhn_sample_brick_trilinear, in cell order for large point sets (same values)."""
+    L = _lib.lib()
+    args = (dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(), dev.ptr(pg), pg.numel(), dev.ptr(pts), n,
+            dev.ptr(out))
+    nbytes = int(L.bhn_sample_sort_scratch_bytes(n, rg.numel() * tg.numel() * pg.numel())) if n >= SORT_MIN_POINTS \
+        else -1
+    if nbytes <= 0:
+        _lib.check(L.bhn_sample_brick_trilinear(*args, dev.stream_ptr()))
+        return
+    scratch = torch.empty(nbytes + 256, dtype=torch.uint8, device=out.device)
+    sp = (dev.ptr(scratch) + 255) & ~255
+    _lib.check(L.bhn_sample_brick_trilinear_sorted(*args, sp, nbytes, dev.stream_ptr()))
 
 
 def sample_brick_valid_mask(r_grid, theta_grid, points):

@@ -77,18 +77,34 @@ __global__ void stokes_exact_brick_kernel(const double *__restrict__ coeffs, int
     }
 }
 
+__device__ __forceinline__ void sample_trilinear_point(const double *__restrict__ coeffs, const double *__restrict__ rg,
+                                                       int nr, const double *__restrict__ tg, int nt,
+                                                       const double *__restrict__ pg, int np,
+                                                       const double *__restrict__ pts, int64_t i,
+                                                       double *__restrict__ out) {
+    double c[11];
+    if (!sample_one_exact(coeffs, rg, nr, tg, nt, pg, np, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], c)) {
+#pragma unroll
+        for (int k = 0; k < 11; ++k) c[k] = __longlong_as_double(0x7ff8000000000000ULL);
+    }
+#pragma unroll
+    for (int k = 0; k < 11; ++k) out[11 * i + k] = c[k];
+}
+
 __global__ void sample_trilinear_kernel(const double *__restrict__ coeffs, const double *__restrict__ rg, int nr,
                                         const double *__restrict__ tg, int nt, const double *__restrict__ pg, int np,
                                         const double *__restrict__ pts, int64_t n, double *__restrict__ out) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double c[11];
-        if (!sample_one_exact(coeffs, rg, nr, tg, nt, pg, np, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], c)) {
-#pragma unroll
-            for (int k = 0; k < 11; ++k) c[k] = __longlong_as_double(0x7ff8000000000000ULL);
-        }
-#pragma unroll
-        for (int k = 0; k < 11; ++k) out[11 * i + k] = c[k];
-    }
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        sample_trilinear_point(coeffs, rg, nr, tg, nt, pg, np, pts, i, out);
+}
+
+__global__ void sample_trilinear_ordered_kernel(const double *__restrict__ coeffs, const double *__restrict__ rg,
+                                                int nr, const double *__restrict__ tg, int nt,
+                                                const double *__restrict__ pg, int np, const double *__restrict__ pts,
+                                                const uint32_t *__restrict__ order, int64_t n,
+                                                double *__restrict__ out) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        sample_trilinear_point(coeffs, rg, nr, tg, nt, pg, np, pts, (int64_t)order[k], out);
 }
 
 __global__ void sample_and_step_kernel(const double *__restrict__ coeffs, const double *__restrict__ rg, int nr,
@@ -468,6 +484,59 @@ SortLayout sort_layout(int64_t n, int64_t cells) {
 
 int64_t bhn_sample_sort_scratch_bytes(int64_t n_points, int64_t cells) { return sort_layout(n_points, cells).total; }
 
+namespace {
+// The cell keys and their radix sort: idx_out (inside the scratch) receives the
+// point indices in cell order.
+int order_points_by_cell(const double *r_grid, int64_t nr, const double *theta_grid, int64_t nt, const double *phi_grid,
+                         int64_t np, const double *points, int64_t n_points, const SortLayout &L, void *scratch,
+                         void *stream, const uint32_t *&idx_out) {
+    unsigned char *base = static_cast<unsigned char *>(scratch);
+    uint32_t *keys_in = reinterpret_cast<uint32_t *>(base + L.keys_in);
+    uint32_t *keys_out = reinterpret_cast<uint32_t *>(base + L.keys_out);
+    uint32_t *idx_in = reinterpret_cast<uint32_t *>(base + L.idx_in);
+    uint32_t *idx_sorted = reinterpret_cast<uint32_t *>(base + L.idx_out);
+    const uint32_t cells = (uint32_t)(nr * nt * np);
+    cudaStream_t s = as_stream(stream);
+    cell_key_kernel<<<grid_for(n_points, 256), 256, 0, s>>>(r_grid, (int)nr, theta_grid, (int)nt, phi_grid, (int)np,
+                                                          points, n_points, cells, keys_in, idx_in);
+    BHN_LAUNCH_CHECK("cell_key_kernel");
+    size_t temp = (size_t)L.temp_bytes;
+    if (cub::DeviceRadixSort::SortPairs(base + L.temp, temp, keys_in, keys_out, idx_in, idx_sorted, (int)n_points, 0,
+                                        key_bits(cells), s) != cudaSuccess)
+        return fail(BHN_ERR_CUDA, "radix sort of the point cells failed");
+    idx_out = idx_sorted;
+    return BHN_OK;
+}
+
+int check_sort_scratch(int64_t n_points, int64_t cells, void *scratch, int64_t scratch_bytes, SortLayout &L) {
+    L = sort_layout(n_points, cells);
+    if (L.total < 0) return fail(BHN_ERR_VALUE, "point count or brick size outside the sorted path's range");
+    if (!scratch || scratch_bytes < L.total || (reinterpret_cast<uintptr_t>(scratch) & 255))
+        return fail(BHN_ERR_VALUE, "scratch must be 256-byte aligned and hold bhn_sample_sort_scratch_bytes bytes");
+    return BHN_OK;
+}
+}  // namespace
+
+int bhn_sample_brick_trilinear_sorted(const double *coeffs, const double *r_grid, int64_t nr, const double *theta_grid,
+                                      int64_t nt, const double *phi_grid, int64_t np, const double *points,
+                                      int64_t n_points, double *out, void *scratch, int64_t scratch_bytes,
+                                      void *stream) {
+    int rc = check_grid_sizes(nr, nt, np);
+    if (rc) return rc;
+    if (n_points < 0) return fail(BHN_ERR_VALUE, "points must contain flat r, theta, phi triples");
+    if (n_points == 0) return BHN_OK;
+    SortLayout L;
+    rc = check_sort_scratch(n_points, nr * nt * np, scratch, scratch_bytes, L);
+    if (rc) return rc;
+    const uint32_t *order = nullptr;
+    rc = order_points_by_cell(r_grid, nr, theta_grid, nt, phi_grid, np, points, n_points, L, scratch, stream, order);
+    if (rc) return rc;
+    sample_trilinear_ordered_kernel<<<grid_for(n_points, 128), 128, 0, as_stream(stream)>>>(
+        coeffs, r_grid, (int)nr, theta_grid, (int)nt, phi_grid, (int)np, points, order, n_points, out);
+    BHN_LAUNCH_CHECK("sample_trilinear_ordered_kernel");
+    return BHN_OK;
+}
+
 int bhn_sample_and_step_stokes_sorted(const double *coeffs, const double *r_grid, int64_t nr,
                                       const double *theta_grid, int64_t nt, const double *phi_grid, int64_t np,
                                       const double *points, int64_t n_points, double ds_cm, const double *initial,
@@ -482,24 +551,13 @@ int bhn_sample_and_step_stokes_sorted(const double *coeffs, const double *r_grid
     if (initial_len != 4 && initial_len != 4 * n_points)
         return fail(BHN_ERR_VALUE, "initial must contain either 4 values or 4 values per sample point");
     if (n_points == 0) return BHN_OK;
-    const int64_t cells = nr * nt * np;
-    const SortLayout L = sort_layout(n_points, cells);
-    if (L.total < 0) return fail(BHN_ERR_VALUE, "point count or brick size outside the sorted path's range");
-    if (!scratch || scratch_bytes < L.total || (reinterpret_cast<uintptr_t>(scratch) & 255))
-        return fail(BHN_ERR_VALUE, "scratch must be 256-byte aligned and hold bhn_sample_sort_scratch_bytes bytes");
-    unsigned char *base = static_cast<unsigned char *>(scratch);
-    uint32_t *keys_in = reinterpret_cast<uint32_t *>(base + L.keys_in);
-    uint32_t *keys_out = reinterpret_cast<uint32_t *>(base + L.keys_out);
-    uint32_t *idx_in = reinterpret_cast<uint32_t *>(base + L.idx_in);
-    uint32_t *idx_out = reinterpret_cast<uint32_t *>(base + L.idx_out);
+    SortLayout L;
+    rc = check_sort_scratch(n_points, nr * nt * np, scratch, scratch_bytes, L);
+    if (rc) return rc;
+    const uint32_t *idx_out = nullptr;
+    rc = order_points_by_cell(r_grid, nr, theta_grid, nt, phi_grid, np, points, n_points, L, scratch, stream, idx_out);
+    if (rc) return rc;
     cudaStream_t s = as_stream(stream);
-    cell_key_kernel<<<grid_for(n_points, 256), 256, 0, s>>>(r_grid, (int)nr, theta_grid, (int)nt, phi_grid, (int)np,
-                                                          points, n_points, (uint32_t)cells, keys_in, idx_in);
-    BHN_LAUNCH_CHECK("cell_key_kernel");
-    size_t temp = (size_t)L.temp_bytes;
-    if (cub::DeviceRadixSort::SortPairs(base + L.temp, temp, keys_in, keys_out, idx_in, idx_out, (int)n_points, 0,
-                                        key_bits((uint32_t)cells), s) != cudaSuccess)
-        return fail(BHN_ERR_CUDA, "radix sort of the point cells failed");
     sample_and_step_ordered_kernel<<<grid_for(n_points, 128), 128, 0, s>>>(
         coeffs, r_grid, (int)nr, theta_grid, (int)nt, phi_grid, (int)np, points, idx_out, n_points, ds_cm, initial,
         initial_len == 4, invalid_policy, out);

@@ -111,6 +111,11 @@ int bhn_sample_and_step_stokes(const double *coeffs, const double *r_grid, int64
  * scratch: bhn_sample_sort_scratch_bytes(n_points, nr * nt * np) bytes,
  * 256-byte aligned, on the device. */
 int64_t bhn_sample_sort_scratch_bytes(int64_t n_points, int64_t cells);
+/* bhn_sample_brick_trilinear in the same cell order (same values, same scratch). */
+int bhn_sample_brick_trilinear_sorted(const double *coeffs, const double *r_grid, int64_t nr, const double *theta_grid,
+                                      int64_t nt, const double *phi_grid, int64_t np, const double *points,
+                                      int64_t n_points, double *out, void *scratch, int64_t scratch_bytes,
+                                      void *stream);
 int bhn_sample_and_step_stokes_sorted(const double *coeffs, const double *r_grid, int64_t nr,
                                       const double *theta_grid, int64_t nt, const double *phi_grid, int64_t np,
                                       const double *points, int64_t n_points, double ds_cm, const double *initial,

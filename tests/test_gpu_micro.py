@@ -160,10 +160,10 @@ def test_throughput_probes_run_and_count():
 
 
 def test_cell_ordered_sampler_equals_the_plain_kernel():
-    """bhn_sample_and_step_stokes_sorted (points taken in brick-cell order,
-    results written to their own rows) gives the plain kernel's bits for every
-    policy, broadcast and per-point initial vectors, points outside the domain,
-    on knots and NaN points."""
+    """bhn_sample_and_step_stokes_sorted and bhn_sample_brick_trilinear_sorted
+    (points taken in brick-cell order, results written to their own rows) give
+    the plain kernels' bits: every policy, broadcast and per-point initial
+    vectors, points outside the domain, on knots and NaN points."""
     import torch
 
     from blackhole_native import _device as dev
@@ -194,6 +194,13 @@ def test_cell_ordered_sampler_equals_the_plain_kernel():
             ordered = torch.empty_like(plain)
             kernels._launch_sample_and_step(c, rg, tg, pg, dp, n, 0.07, ini, policy, ordered)
             assert torch.equal(plain.view(torch.int64), ordered.view(torch.int64)), (per_point, policy)
+    plain = torch.empty(11 * n, dtype=torch.float64, device=device)
+    _lib.check(L.bhn_sample_brick_trilinear(dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(), dev.ptr(pg),
+                                            pg.numel(), dev.ptr(dp), n, dev.ptr(plain), dev.stream_ptr()))
+    ordered = torch.empty_like(plain)
+    kernels._launch_sample_trilinear(c, rg, tg, pg, dp, n, ordered)
+    assert torch.equal(plain.view(torch.int64), ordered.view(torch.int64))
+    plain = torch.empty(4 * n, dtype=torch.float64, device=device)
     assert L.bhn_sample_sort_scratch_bytes(n, b.cells) > 16 * n
     assert L.bhn_sample_sort_scratch_bytes(0, b.cells) == -1 and L.bhn_sample_sort_scratch_bytes(n, 0) == -1
     rc = L.bhn_sample_and_step_stokes_sorted(dev.ptr(c), dev.ptr(rg), rg.numel(), dev.ptr(tg), tg.numel(),
