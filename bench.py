@@ -869,7 +869,7 @@ def bench_bricks(args) -> dict | None:
     value = sum_over_ranks(pixels * args.steps, world, device) / (t_max * 1e-3)
 
     e2e = None
-    if not args.no_e2e:  # public API: host brick in (float32, converted and uploaded), host image out
+    if not args.no_e2e:  # public API: host brick in (float32, uploaded and widened on the device), host image out
         ke = max(1, min(args.steps, 3))
         barrier(world)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -882,7 +882,7 @@ def bench_bricks(args) -> dict | None:
         barrier(world)
         te = max_over_ranks(a0.elapsed_time(a1), world, device)
         assert np.array_equal(host, img.cpu().numpy()), "public-API image differs from the device launch"
-        h2d = int(b.coeffs.size * 8 + (b.r.size + b.theta.size + b.phi.size) * 8)
+        h2d = int(b.coeffs.nbytes + (b.r.size + b.theta.size + b.phi.size) * 8)  # the brick in its own dtype
         e2e = {"value": sum_over_ranks(pixels * ke, world, device) / (te * 1e-3), "unit": "pixels/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(pixels * 4 * 8), "ms_per_step": te / ke,
                "api": "render_stokes_image_bricks"}

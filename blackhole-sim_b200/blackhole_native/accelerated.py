@@ -93,7 +93,10 @@ class DeviceBricks:
             raise ValueError("coefficient brick contains non-finite values")
         self.device = device or dev.require_cuda()
         self.grids = [torch.as_tensor(g, device=self.device) for g in host_grids]
-        self.coeffs = torch.as_tensor(np.ascontiguousarray(coeffs, dtype=np.float64), device=self.device)
+        # uploaded in the brick's own dtype and widened to float64 on the device (exact)
+        src = np.ascontiguousarray(coeffs if coeffs.dtype in (np.float16, np.float32, np.float64) else
+                                   coeffs.astype(np.float64))
+        self.coeffs = torch.from_numpy(src).to(self.device).to(torch.float64)
 
 
 def _view_and_config(cfg, snapshot, tile):
