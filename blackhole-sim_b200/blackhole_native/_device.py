@@ -42,6 +42,24 @@ def to_device(a: np.ndarray, device: torch.device) -> torch.Tensor:
     return t.to(device, non_blocking=True)
 
 
+def to_device_many(arrays, device: torch.device) -> list[torch.Tensor]:
+    """Several float64 host arrays -> device tensors.  Up to 8 MB together they
+    go in one host-to-device copy, packed back to back (each start 32-byte
+    aligned) and returned as views of one device buffer."""
+    flats = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in arrays]
+    if sum(f.nbytes for f in flats) > (8 << 20):  # large inputs: one copy each, no host repacking
+        return [to_device(f, device) for f in flats]
+    offs, total = [], 0
+    for f in flats:
+        offs.append(total)
+        total += -(-f.size // 4) * 4
+    host = np.empty(max(total, 1), dtype=np.float64)
+    for f, o in zip(flats, offs):
+        host[o:o + f.size] = f
+    buf = to_device(host, device)
+    return [buf[o:o + f.size] for f, o in zip(flats, offs)]
+
+
 def check_values_device(t: torch.Tensor, increasing: bool) -> tuple[int, int]:
     """(non-finite count, non-increasing neighbour count) of a float64 device tensor."""
     counts = torch.zeros(2, dtype=torch.int32, device=t.device)

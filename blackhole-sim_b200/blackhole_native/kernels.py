@@ -144,7 +144,7 @@ def _stokes_brick(coeffs, ds_cm, initial, entry):
     if not np.all(np.isfinite(ini)):
         raise ValueError("initial must contain only finite values")
     device = dev.require_cuda()
-    dc, di = dev.to_device(c, device), dev.to_device(ini, device)
+    dc, di = dev.to_device_many((c, ini), device)
     out = torch.empty(cells * STOKES_COMPONENTS, dtype=torch.float64, device=device)
     _lib.check(getattr(_lib.lib(), entry)(dev.ptr(dc), cells, ds, dev.ptr(di), ini.size, dev.ptr(out),
                                           dev.stream_ptr()))
@@ -166,7 +166,7 @@ def sample_brick_trilinear(coeffs, r_grid, theta_grid, phi_grid, points):
     c, rg, tg, pg, pts = (dev.host_f64(x) for x in (coeffs, r_grid, theta_grid, phi_grid, points))
     n = _validate_sampler_host(c, rg, tg, pg, pts)
     device = dev.require_cuda()
-    d = [dev.to_device(x, device) for x in (c, rg, tg, pg, pts)]
+    d = dev.to_device_many((c, rg, tg, pg, pts), device)
     out = torch.empty(n * COEFFS_PER_CELL, dtype=torch.float64, device=device)
     _launch_sample_trilinear(*d, n, out)
     return out.cpu().numpy().tolist()
@@ -204,7 +204,7 @@ def sample_and_step_stokes(coeffs, r_grid, theta_grid, phi_grid, points, ds_cm, 
     if not np.all(np.isfinite(ini)):
         raise ValueError("initial must contain only finite values")
     device = dev.require_cuda()
-    d = [dev.to_device(x, device) for x in (c, rg, tg, pg, pts, ini)]
+    d = dev.to_device_many((c, rg, tg, pg, pts, ini), device)
     out = torch.empty(n * STOKES_COMPONENTS, dtype=torch.float64, device=device)
     _launch_sample_and_step(*d[:5], n, ds, d[5], policy, out)
     return out.cpu().numpy().tolist()
@@ -271,7 +271,7 @@ def sample_brick_valid_mask(r_grid, theta_grid, points):
         raise ValueError("points must contain only finite values")
     n = pts.size // 3
     device = dev.require_cuda()
-    d = [dev.to_device(x, device) for x in (rg, tg, pts)]
+    d = dev.to_device_many((rg, tg, pts), device)
     mask = torch.empty(n, dtype=torch.uint8, device=device)
     _lib.check(_lib.lib().bhn_sample_brick_valid_mask(dev.ptr(d[0]), rg.size, dev.ptr(d[1]), tg.size, dev.ptr(d[2]),
                                                       n, dev.ptr(mask), dev.stream_ptr()))
