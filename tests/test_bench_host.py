@@ -33,8 +33,23 @@ def test_bricks_cpu_baseline_contract():
 def test_bench_lists_the_bricks_workload():
     out = subprocess.run([sys.executable, str(REPO / "bench.py"), "--help"], capture_output=True, text=True,
                          check=True).stdout
-    assert "bricks" in out and "--workload" in out
+    assert "bricks" in out and "micro" in out and "--workload" in out
     import bench
 
     assert bench.FP64_FLOP_PER_RK4_STEP > 4 * 100 and bench.FP64_FLOP_PER_SEGMENT > 7 * 11 * 3
     json.dumps(bench.BRICKS_BRICK)
+
+
+def test_micro_cpu_baseline_contract():
+    sys.path.insert(0, str(REPO))
+    import bench
+    from blackhole_native import bricks
+
+    b = bricks.torus_brick(8, 6, 8, spin_a=0.9375, seed=0, dtype=np.float64)
+    rng = np.random.default_rng(1)
+    pts = np.stack([rng.uniform(b.r[0], b.r[-1], 5000), rng.uniform(b.theta[0], b.theta[-1], 5000),
+                    rng.uniform(0.0, 6.28, 5000)], axis=1)
+    out = bench.micro_cpu_baseline(b, pts, 0.05, target_s=0.05)
+    assert set(out) == {"value", "unit", "cores", "kind", "sample"}
+    assert out["unit"] == "points/s" and out["cores"] == 1 and out["value"] > 0
+    assert bench.MICRO_BYTES_PER_POINT == 3 * 8 + 8 * 11 * 8 + 4 * 8
