@@ -1024,11 +1024,35 @@ def bench_micro(args) -> dict | None:
                "ms_per_step": te / ke, "api": "sample_and_step_stokes (numpy in, list out)",
                "points_per_step": ne}
 
+    # stokes_rk2_brick (lib.rs:210-279) over the whole brick: a streaming kernel,
+    # 88 B of coefficients in and 32 B of Stokes out per cell
+    from blackhole_native import _device as dev
+    from blackhole_native import _lib
+
+    cells = int(b.cells)
+    rk_out = torch.empty(4 * cells, dtype=torch.float64, device=device)
+    rk_ref = kernels.stokes_rk2_brick(c, M["ds_cm"], ini)  # the checked public tensor call
+
+    def rk2():
+        _lib.check(_lib.lib().bhn_stokes_rk2_brick(dev.ptr(c), cells, M["ds_cm"], dev.ptr(ini), 4, dev.ptr(rk_out),
+                                                   stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        rk2()
+    rk_per = timed_launches(rk2, args.steps, stream, device)
+    assert torch.equal(rk_out, rk_ref)
+    rk_ms = statistics.mean(rk_per)
+    rk_gbs = 120.0 * cells / (rk_ms * 1e-3) / 1e9
+    peaks = load_peaks()
+    stokes_rk2 = {"cells_per_step": cells, "ms_per_step": rk_ms, "cells_per_s": cells / (rk_ms * 1e-3),
+                  "roofline": {"bound": "hbm", "achieved": round(rk_gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                               "frac": round(rk_gbs / peaks["hbm_gbs"], 4), "kernel": "stokes_rk2_brick_kernel",
+                               "algorithmic_bytes_per_cell": 120}}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = micro_cpu_baseline(b, pts, M["ds_cm"], args.cpu_seconds)
     per_mean = statistics.mean(per)
-    peaks = load_peaks()
     achieved = MICRO_BYTES_PER_POINT * n / (per_mean * 1e-3) / 1e9
     line = {
         "metric": "points/s", "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
@@ -1049,6 +1073,7 @@ def bench_micro(args) -> dict | None:
                                "sampler)", "algorithmic_bytes_per_point": MICRO_BYTES_PER_POINT},
         "cpu_baseline": cpu,
         "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
+        "stokes_rk2_brick": stokes_rk2,
     }
     if world > 1:
         import torch.distributed as td
