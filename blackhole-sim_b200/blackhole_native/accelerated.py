@@ -211,7 +211,8 @@ def sample_coefficient_brick(bricks, r: float, theta: float, phi: float) -> np.n
 
 @dataclass(frozen=True)
 class ImageRegressionMetrics:
-    """webgpu_regression.py:27-36."""
+    """The fields of the reference's ImageRegressionMetrics
+    (webgpu_regression.py:27-36) and its default pass thresholds."""
 
     max_abs: float
     mean_abs: float
@@ -225,18 +226,23 @@ class ImageRegressionMetrics:
 
 
 def image_metrics(candidate, reference) -> ImageRegressionMetrics:
-    """webgpu_regression.py:39-48 (host arithmetic on two images)."""
+    """Regression metrics of a candidate image against a reference image, as
+    the reference's regression test defines them (webgpu_regression.py:39-48):
+    the largest and the mean absolute difference, the RMSE, the PSNR for a
+    unit peak (the RMSE floored at 1e-300), and a SHA-256 fingerprint of the
+    candidate's float32 bytes.  Host arithmetic on two small images."""
     import hashlib
 
-    a = np.asarray(candidate, dtype=float)
-    b = np.asarray(reference, dtype=float)
-    if a.shape != b.shape:
-        raise ValueError(f"shape mismatch: {a.shape} vs {b.shape}")
-    diff = np.abs(a - b)
-    rmse = float(np.sqrt(np.mean((a - b) ** 2)))
-    psnr = float(20.0 * np.log10(1.0 / max(rmse, 1.0e-300)))
-    digest = hashlib.sha256(np.asarray(candidate, dtype=np.float32).tobytes()).hexdigest()
-    return ImageRegressionMetrics(float(np.max(diff)), float(np.mean(diff)), rmse, psnr, digest)
+    cand = np.asarray(candidate, dtype=np.float64)
+    ref = np.asarray(reference, dtype=np.float64)
+    if cand.shape != ref.shape:
+        raise ValueError(f"shape mismatch: {cand.shape} vs {ref.shape}")
+    err = np.subtract(cand, ref)
+    magnitude = np.abs(err)
+    rmse = float(np.sqrt(np.square(err).mean()))
+    fingerprint = hashlib.sha256(cand.astype(np.float32).tobytes()).hexdigest()
+    return ImageRegressionMetrics(max_abs=float(magnitude.max()), mean_abs=float(magnitude.mean()), rmse=rmse,
+                                  psnr_db=float(20.0 * np.log10(1.0 / max(rmse, 1.0e-300))), sha256=fingerprint)
 
 
 @dataclass(frozen=True)

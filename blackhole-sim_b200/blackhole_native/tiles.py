@@ -1,7 +1,8 @@
 """Tiled and progressive (coarse-to-fine) rendering.
 
 ``generate_tiles`` / ``progressive_levels`` / ``generate_progressive_tiles``
-mirror the reference's scheduling helpers (python/blackhole_sim/tiles.py:9-59).
+give the same tiles and levels as the reference's scheduling helpers
+(python/blackhole_sim/tiles.py:9-57).
 ``progressive_render`` is their GPU use: every level of the coarse-to-fine
 ladder is one persistent launch on the current stream, queued back to back,
 and each level's image is handed out as soon as its own launch has finished
@@ -11,6 +12,8 @@ levels still render.
 
 from __future__ import annotations
 
+import itertools
+import math
 from dataclasses import dataclass, replace
 from typing import Iterator, Sequence
 
@@ -21,7 +24,10 @@ from .render import DeviceBrick, RenderConfig, Renderer, View
 
 @dataclass(frozen=True, order=True)
 class RenderTile:
-    """tiles.py:9-27."""
+    """One rectangle [x0, x1) x [y0, y1) of the image at a progressive level.
+
+    Field order and ordering are the reference's (python/blackhole_sim/tiles.py:9-27):
+    tiles sort by level, then row, then column."""
 
     level: int
     y0: int
@@ -42,36 +48,41 @@ class RenderTile:
         return self.width * self.height
 
 
+def _spans(extent: int, size: int) -> list[tuple[int, int]]:
+    """[start, stop) pieces of at most ``size`` covering range(extent)."""
+    starts = range(0, int(extent), int(size))
+    return [(s, min(s + size, extent)) for s in starts]
+
+
 def generate_tiles(width: int, height: int, tile_size: int = 64, level: int = 0) -> list[RenderTile]:
-    """tiles.py:30-35: row-major tiles of at most tile_size pixels a side."""
-    tiles: list[RenderTile] = []
-    for y in range(0, int(height), int(tile_size)):
-        for x in range(0, int(width), int(tile_size)):
-            tiles.append(RenderTile(level, x0=x, y0=y, x1=min(x + tile_size, width), y1=min(y + tile_size, height)))
-    return tiles
+    """Row-major tiles of at most ``tile_size`` pixels a side covering a
+    width x height image; edge tiles are clipped (tiles.py:30-35)."""
+    rows, cols = _spans(height, tile_size), _spans(width, tile_size)
+    return [RenderTile(level, y0=y0, x0=x0, x1=x1, y1=y1) for (y0, y1), (x0, x1) in itertools.product(rows, cols)]
 
 
 def progressive_levels(width: int, height: int, min_width: int = 480) -> list[tuple[int, int, int]]:
-    """tiles.py:38-51: (level, width, height) from the coarsest power-of-two
-    reduction at least min_width wide up to the full image."""
-    out: list[tuple[int, int, int]] = []
-    w = int(width)
-    scale = 1
-    while w // (scale * 2) >= min_width:
-        scale *= 2
-    level = 0
-    while scale >= 1:
-        out.append((level, max(1, width // scale), max(1, height // scale)))
-        level += 1
-        scale //= 2
-    return out
+    """(level, width, height) of the coarse-to-fine ladder (tiles.py:38-51).
+
+    Level 0 is the image reduced by 2**k, k the largest power whose reduced
+    width ``width // 2**k`` is still at least ``min_width`` (k = 0 when the
+    image is narrower than that); every further level halves the reduction,
+    the last being the full image.  ``width // 2**k >= m`` holds exactly when
+    2**k <= width // ceil(m), so k is the bit length of that quotient less one.
+    """
+    m = math.ceil(min_width)
+    if m < 1:
+        raise ValueError("min_width must be at least 1")
+    quotient = int(width) // m
+    k = quotient.bit_length() - 1 if quotient >= 1 else 0
+    return [(level, max(1, width // 2 ** (k - level)), max(1, height // 2 ** (k - level))) for level in range(k + 1)]
 
 
 def generate_progressive_tiles(width: int, height: int, tile_size: int = 64,
                                min_width: int = 480) -> Iterator[RenderTile]:
-    """tiles.py:54-57."""
-    for level, w, h in progressive_levels(width, height, min_width):
-        yield from generate_tiles(w, h, tile_size, level)
+    """The tiles of every progressive level, coarsest level first (tiles.py:54-57)."""
+    return itertools.chain.from_iterable(generate_tiles(w, h, tile_size, level)
+                                         for level, w, h in progressive_levels(width, height, min_width))
 
 
 def tile_views(view: View, tiles: Sequence[RenderTile]) -> list[View]:

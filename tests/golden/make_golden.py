@@ -1,8 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container where the reference project is mounted (read-only):
+Run where a copy of the reference project is readable, naming its python/
+directory (or setting BHN_REFERENCE_PYTHON to it):
 
-    python tests/golden/make_golden.py --reference /root/reference/python
+    python tests/golden/make_golden.py --reference <reference project>/python
 
 Every output value in the fixtures is computed by the reference's own Python
 functions (python/blackhole_sim/native_kernels.py, kerr.py,
@@ -18,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import math
+import os
 import sys
 import time
 from pathlib import Path
@@ -492,7 +494,9 @@ def accel_regression_fixtures(grmhd, calibration, cb, acc, pr, physics) -> dict[
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference/python")
+    env_ref = os.environ.get("BHN_REFERENCE_PYTHON")
+    ap.add_argument("--reference", default=env_ref, required=env_ref is None,
+                    help="the reference project's python/ directory (default: $BHN_REFERENCE_PYTHON)")
     ap.add_argument("--only", default="",
                     help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb,accel,accelreg")
     args = ap.parse_args()
