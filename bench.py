@@ -49,6 +49,7 @@ UNIT = "ray-steps/s"
 WORKLOAD = dict(width=1024, height=1024, spin_a=0.9375, r_obs=1000.0, inclination_deg=17.0, max_steps=4096,
                 h_scale=0.02, h_min=1e-3, h_max=1.0, escape_radius=220.0)
 BRICK = dict(nr=256, ntheta=128, nphi=256, seed=0)
+FOV_Y_DEG = 2.0 * math.degrees(math.atan(20.0 / 1000.0))  # +-20 M at r_obs = 1000 M (the View default)
 # Algorithmic work of the implemented method (counted from the kernel's
 # arithmetic, one FMA = 2 FLOP, a divide / sqrt = 1): a geodesic RK2 step
 # (two Hamiltonian right-hand sides with their pole sin/cos, the FP64 state
@@ -195,20 +196,24 @@ def profiled_traffic(summary: Path = PROFILE_SUMMARY) -> float | None:
     return None
 
 
+def _bricks_module():
+    """blackhole_native/bricks.py loaded by its path: it needs numpy only, and
+    importing the package would load the CUDA library (the reference arm must
+    run without it)."""
+    import importlib.util
+
+    name = "_bhn_bricks_numpy"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, REPO / "blackhole-sim_b200" / "blackhole_native" / "bricks.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
 def make_brick():
-    from blackhole_native import bricks
-
-    return bricks.torus_brick(BRICK["nr"], BRICK["ntheta"], BRICK["nphi"], spin_a=WORKLOAD["spin_a"],
-                              seed=BRICK["seed"], dtype=np.float32)
-
-
-def cpu_sample_view(n: int, **over):
-    from blackhole_native import View
-
-    kw = dict(WORKLOAD)
-    kw.update(width=n, height=n)
-    kw.update(over)
-    return View(**kw)
+    return _bricks_module().torus_brick(BRICK["nr"], BRICK["ntheta"], BRICK["nphi"], spin_a=WORKLOAD["spin_a"],
+                                        seed=BRICK["seed"], dtype=np.float32)
 
 
 def run_oracle(brick, n: int, threads: int = 0) -> tuple[int, float]:
@@ -217,11 +222,11 @@ def run_oracle(brick, n: int, threads: int = 0) -> tuple[int, float]:
     sys.path.insert(0, str(REPO))
     from oracle import oracle as O
 
-    v = cpu_sample_view(n)
-    ov = O.make_view(spin_a=v.spin_a, r_obs=v.r_obs, theta_obs=math.radians(v.inclination_deg), phi_obs=0.0,
-                     fov_y_deg=v.fov_y_deg, roll_deg=0.0, h_scale=v.h_scale, h_min=v.h_min, h_max=v.h_max,
-                     escape_radius=v.escape_radius, affine_to_length_cm=1.0, max_optical_depth=30.0, width=n,
-                     height=n, x0=0, y0=0, crop_w=n, crop_h=n, max_steps=v.max_steps)
+    w = WORKLOAD
+    ov = O.make_view(spin_a=w["spin_a"], r_obs=w["r_obs"], theta_obs=math.radians(w["inclination_deg"]), phi_obs=0.0,
+                     fov_y_deg=FOV_Y_DEG, roll_deg=0.0, h_scale=w["h_scale"], h_min=w["h_min"], h_max=w["h_max"],
+                     escape_radius=w["escape_radius"], affine_to_length_cm=1.0, max_optical_depth=30.0, width=n,
+                     height=n, x0=0, y0=0, crop_w=n, crop_h=n, max_steps=w["max_steps"])
     t0 = time.perf_counter()
     _, steps, _, _ = O.render(ov, brick.coeffs, brick.r, brick.theta, brick.phi, stop_at_tau=True, threads=threads)
     return int(steps.sum()), time.perf_counter() - t0

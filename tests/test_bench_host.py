@@ -53,3 +53,26 @@ def test_micro_cpu_baseline_contract():
     assert set(out) == {"value", "unit", "cores", "kind", "sample"}
     assert out["unit"] == "points/s" and out["cores"] == 1 and out["value"] > 0
     assert bench.MICRO_BYTES_PER_POINT == 3 * 8 + 8 * 11 * 8 + 4 * 8
+
+
+def test_reference_arm_runs_without_the_cuda_library():
+    """The reference arm times the oracle only: it must not import the package
+    (which loads libbhnative.so).  Run on a small brick in a fresh process."""
+    code = (
+        "import sys, json, io, contextlib\n"
+        f"sys.path.insert(0, {str(REPO)!r})\n"
+        "import bench\n"
+        "bench.BRICK.update(nr=16, ntheta=8, nphi=16)\n"
+        "bench.WORKLOAD.update(max_steps=400)\n"
+        "buf = io.StringIO()\n"
+        "with contextlib.redirect_stdout(buf):\n"
+        "    bench.main(['--impl', 'reference', '--steps', '1', '--warmup', '3', '--ref-seconds', '0.1'])\n"
+        "line = json.loads(buf.getvalue().strip().splitlines()[-1])\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'impl': line['impl'], 'value': line['value'], 'pkg': 'blackhole_native' in sys.modules,\n"
+        "                  'so': 'libbhnative' in maps, 'oracle': 'liboracle' in maps}))\n"
+    )
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True, cwd=str(REPO))
+    got = json.loads(out.stdout.strip().splitlines()[-1])
+    assert got["impl"] == "reference" and got["value"] > 0
+    assert got["oracle"] and not got["pkg"] and not got["so"]
