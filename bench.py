@@ -253,6 +253,50 @@ def cpu_baseline(brick, target_s: float = 12.0) -> dict:
                       f"in {dt:.2f} s"}
 
 
+def fp32_peak(device, stream) -> float:
+    """FP32 FMA peak of this GPU in TFLOP/s (the denominator of the FP32
+    roofline), measured with the library's FMA-chain probe."""
+    import ctypes
+
+    import torch
+
+    from blackhole_native import _lib
+
+    probe = torch.empty(1 << 20, dtype=torch.float32, device=device)
+    flops = ctypes.c_int64()
+    L = _lib.lib()
+    for _ in range(2):
+        _lib.check(L.bhn_fp32_peak_probe(probe.data_ptr(), 4096, 8, ctypes.byref(flops), stream.cuda_stream))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _lib.check(L.bhn_fp32_peak_probe(probe.data_ptr(), 4096, 8, ctypes.byref(flops), stream.cuda_stream))
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    return flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+
+def render_rooflines(steps: int, brick_steps: int, rays: int, kernel_s: float, fp32_peak_tflops: float,
+                     traffic: float | None, traffic_source: str | None) -> tuple[dict, dict]:
+    """HBM roofline (algorithmic gather bytes) and FP32 roofline (algorithmic
+    FLOP) of one render launch."""
+    peaks = load_peaks()
+    alg_bytes = brick_steps * BYTES_PER_BRICK_STEP + rays * BYTES_PER_RAY
+    alg_flops = steps * FLOP_PER_STEP + brick_steps * FLOP_PER_BRICK_STEP
+    achieved_gbs = alg_bytes / kernel_s / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved_gbs / peaks["hbm_gbs"], 4), "traffic": traffic,
+                "traffic_source": traffic_source,
+                "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)" if peaks["source"] == "measured"
+                else "fallback 6.65 TB/s",
+                "kernel": "render_kernel<Tracer32>", "algorithmic_bytes_per_launch": int(alg_bytes)}
+    achieved_tf = alg_flops / kernel_s / 1e12
+    roofline_fp32 = {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_peak_tflops, 2),
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_peak_tflops, 4),
+                     "peak_source": "measured in this run (bhn_fp32_peak_probe FMA loop)",
+                     "algorithmic_flops_per_launch": int(alg_flops)}
+    return roofline, roofline_fp32
+
+
 # ------------------------------------------------------------------ arms
 def bench_ours(args) -> dict | None:
     import torch
@@ -285,20 +329,7 @@ def bench_ours(args) -> dict | None:
     rnd = bn.Renderer(db, [view], config=cfg, precision="fp32")
     stream = torch.cuda.current_stream(device)
 
-    # FP32 FMA peak on this GPU (denominator of the FP32 roofline)
-    probe = torch.empty(1 << 20, dtype=torch.float32, device=device)
-    flops = __import__("ctypes").c_int64()
-    L = _lib.lib()
-    for _ in range(2):
-        _lib.check(L.bhn_fp32_peak_probe(probe.data_ptr(), 4096, 8, __import__("ctypes").byref(flops),
-                                         stream.cuda_stream))
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    _lib.check(L.bhn_fp32_peak_probe(probe.data_ptr(), 4096, 8, __import__("ctypes").byref(flops),
-                                     stream.cuda_stream))
-    e1.record(stream)
-    torch.cuda.synchronize(device)
-    fp32_peak_tflops = flops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    fp32_peak_tflops = fp32_peak(device, stream)
 
     rnd.capture()
     for _ in range(args.warmup):
@@ -363,22 +394,13 @@ def bench_ours(args) -> dict | None:
         pipe.release()
         del pinned, host_outs, pipe
 
-    peaks = load_peaks()
     kernel_s = statistics.mean(per_launch_ms) * 1e-3
-    alg_bytes = brick_steps * BYTES_PER_BRICK_STEP + rays * BYTES_PER_RAY
-    alg_flops = steps_per_launch * FLOP_PER_STEP + brick_steps * FLOP_PER_BRICK_STEP
-    achieved_gbs = alg_bytes / kernel_s / 1e9
     traffic = profiled_traffic()
-    roofline = {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved_gbs / peaks["hbm_gbs"], 4), "traffic": traffic,
-                "peak_source": f"{peaks['source']} (MEASURED_PEAKS.json hbm_gbs)" if peaks["source"] == "measured"
-                else "fallback 6.65 TB/s",
-                "kernel": "render_kernel<Tracer32>", "algorithmic_bytes_per_launch": int(alg_bytes)}
-    achieved_tf = alg_flops / kernel_s / 1e12
-    roofline_fp32 = {"bound": "fp32", "achieved": round(achieved_tf, 2), "peak": round(fp32_peak_tflops, 2),
-                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp32_peak_tflops, 4),
-                     "peak_source": "measured in this run (bhn_fp32_peak_probe FMA loop)",
-                     "algorithmic_flops_per_launch": int(alg_flops)}
+    roofline, roofline_fp32 = render_rooflines(
+        steps_per_launch, brick_steps, rays, kernel_s, fp32_peak_tflops,
+        traffic if view.width == 1024 else None,
+        f"not measured in this run: dram__bytes_read.sum + dram__bytes_write.sum of one timed launch of this "
+        f"workload from the ncu capture summarised in {PROFILE_SUMMARY.relative_to(REPO)}" if traffic else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -397,6 +419,13 @@ def bench_ours(args) -> dict | None:
                 view.height // 4)
         accuracy = studies.fine_step_check(db64, view, crop, config=cfg)
         del db64
+
+    # BASELINE's second metric (outside the timed region, rank 0 of a 1-GPU run):
+    # time to a 2048^2 image at <= 1e-3 Stokes-I rel L1, learned step size
+    # against the step-doubling controller and the fastest plain step
+    tti = None
+    if rank == 0 and world == 1 and not args.no_time_to_image:
+        tti = time_to_image(device, 2048, 3)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -417,6 +446,7 @@ def bench_ours(args) -> dict | None:
         "status_counts": st2.status,
         "h_drift": {"max_all_rays": st2.max_h_drift, "max_escaped_rays": st2.max_h_drift_escaped},
         "accuracy": accuracy,
+        "time_to_image": tti,
     }
     rnd.release_graph()
     if world > 1:
@@ -451,6 +481,7 @@ def bench_views(args) -> dict | None:
     cfg = bn.RenderConfig(**args.config) if args.config else (autotune.cached_config(key, device) or bn.RenderConfig())
     rnd = bn.Renderer(db, views, config=cfg, precision="fp32")
     stream = torch.cuda.current_stream(device)
+    fp32_peak_tflops = fp32_peak(device, stream)
     rnd.capture()
     for _ in range(args.warmup):
         rnd.graph_launch()
@@ -458,6 +489,8 @@ def bench_views(args) -> dict | None:
     st = rnd.result().stats()
     K = args.steps
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    clocks = ClockSampler(_uuid(device)).start()
+    time.sleep(0.3)
     barrier(world)
     torch.cuda.synchronize(device)
     evs[0].record(stream)
@@ -466,10 +499,13 @@ def bench_views(args) -> dict | None:
         evs[i + 1].record(stream)
     torch.cuda.synchronize(device)
     barrier(world)
+    clk = clocks.stop()
     total_ms = evs[0].elapsed_time(evs[K])
     t_max = max_over_ranks(total_ms, world, device)
     value = sum_over_ranks(st.ray_steps * K, world, device) / (t_max * 1e-3)
     rnd.release_graph()
+    roofline, roofline_fp32 = render_rooflines(st.ray_steps, st.brick_steps, st.rays, total_ms / K * 1e-3,
+                                               fp32_peak_tflops, None, None)
     # per view, each rendered alone (same launch shape)
     per_view = []
     for v in views:
@@ -483,6 +519,32 @@ def bench_views(args) -> dict | None:
         s1 = r1.result().stats()
         per_view.append(s1.ray_steps / (a.elapsed_time(b) * 1e-3))
     pv = np.asarray(per_view)
+    h_drift = accuracy = cpu = None
+    if rank == 0:
+        from blackhole_native import studies
+
+        # Hamiltonian drift of every ray of the batch (one untimed launch with per-ray outputs)
+        rr = bn.Renderer(db, views, config=cfg, precision="fp32", ray_outputs=True).launch()
+        torch.cuda.synchronize(device)
+        h_drift = studies._drift_summary(rr.h_drift.cpu().numpy().astype(np.float64), rr.status.cpu().numpy())
+        del rr
+        if not args.no_accuracy:
+            # Stokes error against the FP64 kernel at h/4 on centred crops (at most 128^2) of four views
+            db64 = bn.DeviceBrick(scenes.shared_brick(), device=device, precisions=("fp32", "fp64"))
+            per = []
+            for v in views[:4]:
+                w, h = min(v.width, 128), min(v.height, 128)
+                crop = ((v.width - w) // 2, (v.height - h) // 2, w, h)
+                per.append(studies.fine_step_check(db64, v, crop, config=cfg))
+            keys = ("rel_l1_I", "rel_l1_Q", "rel_l1_U", "rel_l1_V", "flux_weighted_dm")
+            accuracy = {"views": [{"side": [v.width, v.height], "spin_a": v.spin_a, "inclination_deg": v.inclination_deg,
+                                   "crop": a["crop"], "mask_fraction": a["mask_fraction"]["fine_step"],
+                                   **a["fp32_vs_fp64_fine"]} for v, a in zip(views[:4], per)],
+                        "max": {k: max(a["fp32_vs_fp64_fine"][k] for a in per) for k in keys},
+                        "fine_step_factor": 0.25}
+            del db64
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = views_cpu_baseline(scenes.shared_brick(), views, args.cpu_seconds)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": t_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -491,18 +553,48 @@ def bench_views(args) -> dict | None:
                                "incl~U(5,85)deg, max_steps~U{512..8192}), shared 128x64x128x11 float32 brick, "
                                "one CUDA-graph launch",
                    "rays_per_step": st.rays, "ray_steps_per_step": st.ray_steps,
+                   "brick_steps_per_step": st.brick_steps,
+                   "l2": "brick records (18 MB) fit in L2; the 1.03e8 rays' Stokes outputs (1.6 GB) do not",
                    "autotune": {"block_threads": cfg.block_threads, "blocks_per_sm": cfg.blocks_per_sm,
                                 "tile": [cfg.tile_w, cfg.tile_h], "refill_min": cfg.refill_min,
                                 "reg_cap": cfg.reg_cap}},
         "per_view_ray_steps_per_s": {"min": float(pv.min()), "median": float(np.median(pv)),
                                      "max": float(pv.max()), "views": len(pv)},
-        "status_counts": st.status, "gpu_launches": K,
+        "status_counts": st.status, "gpu_launches": K, "clocks": clk, "roofline": roofline,
+        "roofline_fp32": roofline_fp32, "cpu_baseline": cpu, "h_drift": h_drift, "accuracy": accuracy,
+        "e2e": None,
     }
     if world > 1:
         import torch.distributed as td
 
         td.destroy_process_group()
     return line if rank == 0 else None
+
+
+def views_cpu_baseline(brick, views, target_s: float) -> dict:
+    """The FP64 oracle (C, OpenMP over every host core) on centred crops of the
+    batch's views, as many views as fit in about target_s seconds."""
+    sys.path.insert(0, str(REPO))
+    from oracle import oracle as O
+
+    steps, spent, used = 0, 0.0, 0
+    for v in views:
+        n = min(24, v.width, v.height)
+        ov = O.make_view(spin_a=v.spin_a, r_obs=v.r_obs, theta_obs=math.radians(v.inclination_deg), phi_obs=0.0,
+                         fov_y_deg=v.fov_y_deg, roll_deg=0.0, h_scale=v.h_scale, h_min=v.h_min, h_max=v.h_max,
+                         escape_radius=v.escape_radius, affine_to_length_cm=1.0, max_optical_depth=30.0,
+                         width=v.width, height=v.height, x0=(v.width - n) // 2, y0=(v.height - n) // 2, crop_w=n,
+                         crop_h=n, max_steps=v.max_steps)
+        t0 = time.perf_counter()
+        _, st, _, _ = O.render(ov, brick.coeffs, brick.r, brick.theta, brick.phi, stop_at_tau=True)
+        spent += time.perf_counter() - t0
+        steps += int(st.sum())
+        used += 1
+        if spent >= target_s:
+            break
+    return {"value": steps / spent, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+            "sample": f"float64 oracle (C, OpenMP): centred 24x24 crops of the first {used} views, {steps} "
+                      f"ray-steps in {spent:.2f} s"}
 
 
 # ------------------------------------------------------------------ synchrotron workloads
@@ -1127,26 +1219,27 @@ def _lib_check(rc):
 
 
 # ------------------------------------------------------------------ learned step size
-def bench_learned(args) -> dict | None:
+FLOP_PER_RHS = 60   # one FP32 Hamiltonian right-hand side with its pole sin / cos (half of a plain step's 213
+                    # less the state update and tests)
+
+
+def time_to_image(device, side: int, reps: int, spin: float = 0.9375, incl: float = 30.0,
+                  cpu_seconds: float = 0.0) -> dict:
     """Time to an image at <= 1e-3 Stokes-I rel L1 against the FP64 kernel at
     h/16: plain fixed-step RK2 at h, h/2, h/4, h/8 against the learned step
-    size and the step-doubling controller, on a 2048x2048 view (a = 0.9375,
-    i = 30 deg, horizon guard on) of a seeded torus brick (seed 1).  The
-    error is taken over pixels whose fine-step result is stable and kept the
-    null constraint (studies.py)."""
+    size and the step-doubling controller, on a side x side view (horizon
+    guard on) of a seeded torus brick (seed 1).  The error is taken over
+    pixels whose fine-step result is stable and kept the null constraint
+    (studies.py).  Each method's time is the fastest of ``reps`` launches
+    (CUDA events); GPU clocks are sampled while the methods run."""
     import torch
 
     from blackhole_native import learned, studies
     from blackhole_native.bricks import torus_brick
     from blackhole_native.render import DeviceBrick, View
 
-    rank, world, local_rank = dist_env()
-    if rank != 0:
-        return None
-    torch.cuda.set_device(local_rank)
-    side = args.side or 2048
-    spin, incl = 0.9375, 30.0
-    db = DeviceBrick(torus_brick(256, 128, 256, spin_a=spin, seed=1), precisions=("fp32", "fp64"))
+    brick = torus_brick(256, 128, 256, spin_a=spin, seed=1)
+    db = DeviceBrick(brick, device=device, precisions=("fp32", "fp64"))
     v = View(side, side, spin_a=spin, inclination_deg=incl, max_steps=65536, horizon_guard=True)
     v16 = v.scaled_step(1 / 16)
     ref_res = studies._render(db, v16, "fp64", ray_outputs=True)[0]
@@ -1162,31 +1255,111 @@ def bench_learned(args) -> dict | None:
     net = learned.shipped_weights()
     if net is None:
         raise RuntimeError("the shipped step-size network (weights/step_net.npz) is missing")
-    reps = max(args.steps, 1)
+    torch.cuda.synchronize(device)
+    clocks = ClockSampler(_uuid(device)).start()
+    time.sleep(0.3)
     runs = {}
     for f in (1.0, 0.5, 0.25, 0.125):
         runs[f"plain h*{f}"] = learned.render_plain(db, [v.scaled_step(f)], repeats=reps)
     runs["learned"] = learned.render_learned(db, [v], net, learned.AdaptConfig(), repeats=reps)
     runs["controller tol 1e-5"] = learned.render_adaptive(db, [v], learned.AdaptConfig(tol=1e-5), repeats=reps)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
     table = {}
     for k, r in runs.items():
         e = studies.image_errors(r.image().cpu().numpy(), ref, mask, scale)
         table[k] = {"ms": round(r.ms, 2), "rel_l1_I": e["rel_l1_I"], "capped_rel_l1_I": e["capped_rel_l1_I"],
-                    "bad_frac": e["bad_frac"], **({"rhs_evals": r.counters["rhs_evals"]} if r.counters else {})}
+                    "rel_l1_Q": e["rel_l1_Q"], "rel_l1_U": e["rel_l1_U"], "rel_l1_V": e["rel_l1_V"],
+                    "flux_weighted_dm": e["flux_weighted_dm"], "bad_frac": e["bad_frac"],
+                    **({"rhs_evals": r.counters["rhs_evals"]} if r.counters else {})}
     ok = {k: t["ms"] for k, t in table.items() if t["rel_l1_I"] <= 1e-3}
     plain_best = min((t for k, t in ok.items() if k.startswith("plain")), default=None)
-    learned_ms = ok.get("learned")
+    plain_key = min((k for k in ok if k.startswith("plain")), key=lambda k: ok[k], default=None)
+    # Hamiltonian drift of the learned loop's rays: one more launch with per-ray outputs
+    lr = learned.render_learned(db, [v], net, learned.AdaptConfig(), repeats=1, ray_outputs=True)
+    h_drift = None
+    if lr.rnd.h_drift is not None:
+        h_drift = studies._drift_summary(lr.rnd.result().per_ray("h_drift").cpu().numpy().astype(np.float64),
+                                         lr.rnd.result().per_ray("status").cpu().numpy())
+    out = {"workload": f"{side}x{side} rays, a={spin}, i={incl}deg, horizon guard, 256x128x256x11 float32 torus "
+                       "brick (seed 1), reference FP64 kernel at h/16",
+           "mask_fraction": float(mask.mean()), "timing": f"each method: the fastest of {reps} launches (CUDA events)",
+           "learned_ms": ok.get("learned"), "controller_ms": ok.get("controller tol 1e-5"),
+           "plain_best_ms": plain_best, "plain_best": plain_key,
+           "speedup_learned_vs_plain": (plain_best / ok["learned"]) if plain_best and ok.get("learned") else None,
+           "speedup_learned_vs_controller": (ok["controller tol 1e-5"] / ok["learned"])
+           if ok.get("controller tol 1e-5") and ok.get("learned") else None,
+           "runs": table, "h_drift_learned": h_drift, "clocks": clk}
+    lrun = runs["learned"]
+    if lrun.counters:
+        tf = lrun.counters["rhs_evals"] * FLOP_PER_RHS / (lrun.ms * 1e-3) / 1e12
+        out["roofline_fp32_learned"] = {
+            "bound": "fp32", "achieved": round(tf, 2), "unit": "TFLOP/s",
+            "note": f"{FLOP_PER_RHS} FP32 FLOP per right-hand-side evaluation x the learned loop's evaluations "
+                    "(brick segments and network not counted)",
+            "peak": round(fp32_peak(device, torch.cuda.current_stream(device)), 2)}
+        out["roofline_fp32_learned"]["frac"] = round(tf / out["roofline_fp32_learned"]["peak"], 4)
+    if cpu_seconds > 0 and plain_key is not None:
+        out["cpu_baseline"] = plain_cpu_time_to_image(brick, v.scaled_step(float(plain_key.split("*")[1])), side,
+                                                      cpu_seconds)
+    return out
+
+
+def plain_cpu_time_to_image(brick, view, side: int, target_s: float) -> dict:
+    """The FP64 oracle (C, OpenMP over every host core) with the plain method
+    at the step that meets the 1e-3 bar on the GPU, on a centred crop sized to
+    about target_s seconds; the time to the full image is extrapolated by the
+    pixel count."""
+    sys.path.insert(0, str(REPO))
+    from oracle import oracle as O
+
+    def run(n):
+        x0 = (side - n) // 2
+        ov = O.make_view(spin_a=view.spin_a, r_obs=view.r_obs, theta_obs=math.radians(view.inclination_deg),
+                         phi_obs=0.0, fov_y_deg=view.fov_y_deg, roll_deg=0.0, h_scale=view.h_scale,
+                         h_min=view.h_min, h_max=view.h_max, escape_radius=view.escape_radius,
+                         affine_to_length_cm=1.0, max_optical_depth=30.0, width=side, height=side, x0=x0, y0=x0,
+                         crop_w=n, crop_h=n, max_steps=view.max_steps, flags=1)  # flags 1: horizon guard
+        t0 = time.perf_counter()
+        O.render(ov, brick.coeffs, brick.r, brick.theta, brick.phi, stop_at_tau=True)
+        return time.perf_counter() - t0
+
+    n = 16
+    dt = run(n)
+    n = int(max(16, min(side, n * math.sqrt(target_s / max(dt, 1e-3)))))
+    dt = run(n)
+    ms = dt * (side * side) / (n * n) * 1e3
+    return {"value": ms, "unit": "ms", "cores": O.max_threads(), "kind": "port",
+            "sample": f"float64 oracle (C, OpenMP), plain RK2 at {view.h_scale:g} r, centred {n}x{n} crop in "
+                      f"{dt:.2f} s, extrapolated to {side}x{side} pixels"}
+
+
+def bench_learned(args) -> dict | None:
+    """BASELINE's second metric on its own line: time to an image at <= 1e-3
+    Stokes-I rel L1, learned step size against plain RK2 and the controller
+    (time_to_image)."""
+    import torch
+
+    rank, world, local_rank = dist_env()
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    side = args.side or 2048
+    reps = max(args.steps, 1)
+    tti = time_to_image(device, side, reps, cpu_seconds=0.0 if args.no_cpu_baseline else args.cpu_seconds)
+    learned_ms = tti["learned_ms"]
     return {
         "metric": "time to an image at <= 1e-3 Stokes-I rel L1 vs the FP64 fine-step kernel (learned step size)",
         "value": learned_ms, "unit": "ms", "n_gpus": 1, "steps": reps, "warmup": None, "ms_per_step": learned_ms,
-        "timing": "each method: the fastest of `steps` launches (CUDA events)",
-        "higher_is_better": False, "scaling": "none", "vs_baseline": None, "dtype": "f32 (BF16 network)",
-        "data": "synthetic",
-        "config": {"workload": f"learned step size: {side}x{side} rays, a={spin}, i={incl}deg, horizon guard, "
-                               "256x128x256x11 float32 torus brick (seed 1), reference FP64 kernel at h/16",
-                   "mask_fraction": float(mask.mean())},
-        "plain_best_ms": plain_best, "speedup_vs_plain": (plain_best / learned_ms) if plain_best and learned_ms else None,
-        "runs": table, "gpu_launches": len(runs) * reps,
+        "timing": tti["timing"], "higher_is_better": False, "scaling": "none", "vs_baseline": None,
+        "dtype": "f32 (BF16 network)", "data": "synthetic",
+        "config": {"workload": "learned step size: " + tti["workload"], "mask_fraction": tti["mask_fraction"]},
+        "plain_best_ms": tti["plain_best_ms"], "speedup_vs_plain": tti["speedup_learned_vs_plain"],
+        "speedup_vs_controller": tti["speedup_learned_vs_controller"], "controller_ms": tti["controller_ms"],
+        "runs": tti["runs"], "gpu_launches": len(tti["runs"]) * reps, "clocks": tti["clocks"],
+        "roofline": tti.get("roofline_fp32_learned"), "cpu_baseline": tti.get("cpu_baseline"),
+        "h_drift": tti["h_drift_learned"],
     }
 
 
@@ -1230,6 +1403,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-time-to-image", action="store_true",
+                    help="skip the learned-vs-controller-vs-plain time to a 2048^2 image at 1e-3")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the crop check against the FP64 kernel at a quarter of the step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU-baseline sample")

@@ -25,8 +25,9 @@ from .kernels import (sample_and_step_stokes, sample_brick_trilinear, sample_bri
 from .render import (DeviceBrick, PipelinedRenderer, RenderConfig, Renderer, RenderResult, RenderStats, View, render,
                      render_stokes)
 from . import accelerated, grrt, tiles
-from .synchrotron import (HybridSynchrotronCoefficients, NonthermalPowerLawSynchrotronCoefficients,
-                          ThermalSynchrotronCoefficients, precompute_coefficient_bricks, precompute_device_brick)
+from .synchrotron import (HybridSynchrotronCoefficients, LocalPlasmaFrame, NonthermalPowerLawSynchrotronCoefficients,
+                          PolarizedCoefficients, ThermalSynchrotronCoefficients, precompute_coefficient_bricks,
+                          precompute_device_brick)
 
 _lib.lib()  # fail loudly at import when the CUDA library is missing
 
@@ -36,7 +37,8 @@ __all__ = [
     "DeviceBrick",
     "RenderConfig", "Renderer", "RenderResult", "RenderStats", "View", "render", "render_stokes", "PipelinedRenderer",
     "precompute_coefficient_bricks", "precompute_device_brick", "HybridSynchrotronCoefficients",
-    "ThermalSynchrotronCoefficients", "NonthermalPowerLawSynchrotronCoefficients", "accelerated", "grrt", "tiles",
+    "ThermalSynchrotronCoefficients", "NonthermalPowerLawSynchrotronCoefficients", "LocalPlasmaFrame",
+    "PolarizedCoefficients", "accelerated", "grrt", "tiles",
 ]
 
 

@@ -26,7 +26,8 @@ EXPORTED = (
     "bhn_render_scratch_bytes", "bhn_render_prepare", "bhn_render_launch", "bhn_render_noalloc",
     "bhn_graph_create", "bhn_graph_launch", "bhn_graph_destroy",
     "bhn_mlp_param_count", "bhn_mlp_blob_bytes", "bhn_mlp_pack", "bhn_mlp_grad", "bhn_mlp_adam", "bhn_mlp_infer",
-    "bhn_adaptive_launch", "bhn_learned_launch", "bhn_brick_precompute", "bhn_grrt_scratch_bytes", "bhn_grrt_render", "bhn_brick_trace_render",
+    "bhn_adaptive_launch", "bhn_learned_launch", "bhn_brick_precompute", "bhn_synchrotron_coefficients",
+    "bhn_grrt_scratch_bytes", "bhn_grrt_render", "bhn_brick_trace_render",
 )
 NOALLOC_MAX_VIEWS = 120  # BHN_NOALLOC_MAX_VIEWS
 

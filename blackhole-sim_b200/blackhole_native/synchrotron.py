@@ -30,8 +30,114 @@ from .bricks import BrickGrid
 from .render import DeviceBrick
 
 
+FRAME_FIELDS = ("n_e_cm3", "theta_e", "b_gauss", "cos_pitch_to_los", "evpa_rad")
+
+
 @dataclass(frozen=True)
-class ThermalSynchrotronCoefficients:
+class LocalPlasmaFrame:
+    """The plasma quantities a coefficient model reads (the fields of
+    synchrotron.py:28-44): electron density [cm^-3], dimensionless electron
+    temperature, field strength [G], cosine of the field's pitch to the line
+    of sight, and the EVPA the linear terms are rotated by."""
+
+    n_e_cm3: float
+    theta_e: float
+    b_gauss: float
+    cos_pitch_to_los: float = 0.0
+    evpa_rad: float = 0.0
+
+    @property
+    def b_perp_gauss(self) -> float:
+        return abs(self.b_gauss) * float(np.sqrt(max(0.0, 1.0 - self.cos_pitch_to_los ** 2)))
+
+    @property
+    def b_parallel_gauss(self) -> float:
+        return self.b_gauss * self.cos_pitch_to_los
+
+
+@dataclass(frozen=True)
+class PolarizedCoefficients:
+    """The 11 polarized transfer coefficients of one frame, fields named and
+    ordered as the reference's PolarizedCoefficients (synchrotron.py:47-64),
+    which is the brick's COEFF_NAMES order."""
+
+    j_i: float = 0.0
+    j_q: float = 0.0
+    j_u: float = 0.0
+    j_v: float = 0.0
+    alpha_i: float = 0.0
+    alpha_q: float = 0.0
+    alpha_u: float = 0.0
+    alpha_v: float = 0.0
+    rho_v: float = 0.0
+    rho_q: float = 0.0
+    rho_u: float = 0.0
+
+    def as_array(self) -> np.ndarray:
+        return np.array([getattr(self, f) for f in self.__dataclass_fields__], dtype=np.float64)
+
+    def as_emission_vector(self) -> np.ndarray:
+        return self.as_array()[:4]
+
+    def propagation_matrix(self) -> np.ndarray:
+        """K of dS/ds = j - K S: alpha_I on the diagonal, the alphas in the first
+        row and column, the rotativities in the symmetric-antisymmetric lower
+        block (the matrix of synchrotron.py:82-94)."""
+        ai, aq, au, av, rv, rq, ru = self.as_array()[4:]
+        k = np.diag([ai, ai, ai, ai])
+        k[0, 1:] = k[1:, 0] = (aq, au, av)
+        k[1, 2], k[2, 1] = rv, -rv
+        k[1, 3], k[3, 1] = -ru, ru
+        k[2, 3], k[3, 2] = rq, -rq
+        return k
+
+
+def _frames_array(frames) -> np.ndarray:
+    """(n, 5) float64 frames from LocalPlasmaFrame-like objects or an array."""
+    if hasattr(frames, "n_e_cm3"):
+        frames = [frames]
+    if isinstance(frames, (list, tuple)) and frames and hasattr(frames[0], "n_e_cm3"):
+        return np.array([[float(getattr(f, k)) for k in FRAME_FIELDS] for f in frames], dtype=np.float64)
+    a = np.ascontiguousarray(np.asarray(frames, dtype=np.float64))
+    if a.ndim == 1 and a.size == 5:
+        a = a.reshape(1, 5)
+    if a.ndim != 2 or a.shape[1] != 5:
+        raise ValueError("frames must be LocalPlasmaFrame objects or an (n, 5) array of "
+                         "(n_e_cm3, theta_e, b_gauss, cos_pitch_to_los, evpa_rad)")
+    return a
+
+
+class _DeviceCoefficients:
+    """Per-frame coefficients of a model on the GPU (``bhn_synchrotron_coefficients``)."""
+
+    def coefficients_batch(self, frames, nu_hz: float):
+        """(n, 11) coefficients for n frames.  ``frames`` is an (n, 5) array or
+        a list of frames (host: a numpy array is returned) or an (n, 5) float64
+        CUDA tensor (the result stays on the device)."""
+        on_device = isinstance(frames, torch.Tensor) and frames.is_cuda
+        if on_device:
+            if frames.dtype != torch.float64 or frames.dim() != 2 or frames.shape[1] != 5:
+                raise ValueError("device frames must be an (n, 5) float64 tensor")
+            fd = frames.contiguous()
+        else:
+            fd = dev.to_device(_frames_array(frames), dev.require_cuda())
+        n = fd.numel() // 5
+        if n < 1:
+            raise ValueError("at least one plasma frame is required")
+        out = torch.empty((n, 11), dtype=torch.float64, device=fd.device)
+        m = model_struct(self, nu_hz, _UNIT_SCALING)
+        _lib.check(_declare_frames().bhn_synchrotron_coefficients(dev.ptr(fd), n, ctypes.byref(m), dev.ptr(out),
+                                                                  dev.stream_ptr()))
+        return out if on_device else out.cpu().numpy()
+
+    def coefficients(self, frame, nu_hz: float) -> PolarizedCoefficients:
+        """The model's coefficients for one frame (the reference's
+        ``coefficients(frame, nu_hz)``), evaluated on the GPU."""
+        return PolarizedCoefficients(*self.coefficients_batch([frame], nu_hz)[0].tolist())
+
+
+@dataclass(frozen=True)
+class ThermalSynchrotronCoefficients(_DeviceCoefficients):
     """synchrotron.py:240-275 (Maxwell-Juettner electrons)."""
 
     gamma_grid_size: int = 192
@@ -41,7 +147,7 @@ class ThermalSynchrotronCoefficients:
 
 
 @dataclass(frozen=True)
-class NonthermalPowerLawSynchrotronCoefficients:
+class NonthermalPowerLawSynchrotronCoefficients(_DeviceCoefficients):
     """synchrotron.py:278-311 (power-law electrons)."""
 
     p: float = 3.5
@@ -55,12 +161,21 @@ class NonthermalPowerLawSynchrotronCoefficients:
 
 
 @dataclass(frozen=True)
-class HybridSynchrotronCoefficients:
+class HybridSynchrotronCoefficients(_DeviceCoefficients):
     """synchrotron.py:314-325: the sum of a thermal and a power-law component."""
 
     thermal: ThermalSynchrotronCoefficients = field(default_factory=ThermalSynchrotronCoefficients)
     nonthermal: NonthermalPowerLawSynchrotronCoefficients = field(
         default_factory=NonthermalPowerLawSynchrotronCoefficients)
+
+
+class _UnitScaling:  # the per-frame models read no plasma scaling
+    rho_cgs_per_code = 1.0
+    b_gauss_per_code = 1.0
+    mean_molecular_weight_per_electron = 1.0
+
+
+_UNIT_SCALING = _UnitScaling()
 
 
 class ModelStruct(ctypes.Structure):
@@ -93,6 +208,15 @@ def _declare() -> ctypes.CDLL:
     fn = L.bhn_brick_precompute
     vp = ctypes.c_void_p
     fn.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.POINTER(ModelStruct), vp, ctypes.c_int32, vp]
+    fn.restype = ctypes.c_int
+    return L
+
+
+def _declare_frames() -> ctypes.CDLL:
+    L = _lib.lib()
+    fn = L.bhn_synchrotron_coefficients
+    vp = ctypes.c_void_p
+    fn.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ModelStruct), vp, vp]
     fn.restype = ctypes.c_int
     return L
 

@@ -686,6 +686,8 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
             const CameraRay cam = camera_ray(v, px.px, px.py);
             const float pt = (float)cam.pt, pphi = (float)cam.pphi;
             Geo g = camera_geo(v, cam);
+            const float H0 = (float)cam.H0;
+            float drift = 0.0f;  // max | |H| - |H0| | over the accepted steps' starts (kerr.py:352, 367)
             StokesAcc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
             // first trial step 0.05 r: the controller then tracks the accepted step
             // without a long ramp from a small start (which would dominate the samples)
@@ -698,6 +700,7 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
                 }
                 Deriv32 k1;
                 rk2_k1(g, C, pt, pphi, k1);
+                drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
                 h = fmaxf(brick_limit(h, g, k1, C, T, P.nr, P.nt, L.A.brick_scale), L.A.h_floor);
                 if (crosses_horizon(g, C, h, k1)) {
                     st = BHN_RAY_CAPTURED;
@@ -735,6 +738,7 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
             write_stokes(P.out, (uint32_t)px.out_idx, acc);
             if (P.ray_steps) P.ray_steps[px.out_idx] = steps;
             if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)st;
+            if (P.ray_drift) P.ray_drift[px.out_idx] = drift;
         }
         __syncwarp();
     }
@@ -778,7 +782,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
         px.px = px.py = 0;
         px.out_idx = 0;
         Geo g = {1000.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        float pt = -1.0f, pphi = 0.0f, mult = 1.0f;
+        float pt = -1.0f, pphi = 0.0f, mult = 1.0f, H0 = 0.0f, drift = 0.0f;
         StokesAcc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
         int steps = 0, st = -1;
         if (alive) {
@@ -788,6 +792,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
             const CameraRay cam = camera_ray(v, px.px, px.py);
             pt = (float)cam.pt;
             pphi = (float)cam.pphi;
+            H0 = (float)cam.H0;
             g = camera_geo(v, cam);
             if (!(v.valid && v.max_steps > 0)) alive = false, st = v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID;
         }
@@ -814,6 +819,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
             float h = fminf(fmaxf(fmaxf(mult, L.A.min_scale) * h_plain, L.A.h_floor), L.A.h_ceil);
             Deriv32 k1, k2;
             rk2_k1(g, C, pt, pphi, k1);
+            drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
             h = fmaxf(brick_limit(h, g, k1, C, T, P.nr, P.nt, L.A.brick_scale), L.A.h_floor);
             if (crosses_horizon(g, C, h, k1)) {
                 st = BHN_RAY_CAPTURED;
@@ -863,6 +869,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
             write_stokes(P.out, (uint32_t)px.out_idx, acc);
             if (P.ray_steps) P.ray_steps[px.out_idx] = steps;
             if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)st;
+            if (P.ray_drift) P.ray_drift[px.out_idx] = drift;
         }
         __syncwarp();
     }
@@ -914,7 +921,7 @@ static int learn_params(const void *records, const void *tables, int32_t nr, int
     P.out = out;
     P.ray_steps = ray_out ? ray_out->steps : nullptr;
     P.ray_status = ray_out ? ray_out->status : nullptr;
-    P.ray_drift = nullptr;
+    P.ray_drift = ray_out ? ray_out->h_drift : nullptr;
     P.tile_w = cfg->tile_w;
     P.tile_h = cfg->tile_h;
     P.refill_min = 32;

@@ -64,6 +64,41 @@ __global__ void __launch_bounds__(128, 6) precompute_kernel(const __grid_constan
     }
 }
 
+// The model's coefficients for given local plasma frames (synchrotron.py:248,
+// :290, :318 -- ThermalSynchrotronCoefficients / NonthermalPowerLaw... /
+// HybridSynchrotronCoefficients.coefficients(frame, nu_hz)): one warp per
+// frame, frames[5 i .. 5 i + 4] = (n_e [cm^-3], Theta_e, B [G], cos of the pitch
+// to the line of sight, EVPA), out[11 i .. 11 i + 10] in PolarizedCoefficients
+// field order (the brick's COEFF_NAMES order).  Theta_e is taken as given: the
+// reference's models floor it only where they divide by it.
+struct FrameParams {
+    Model M;
+    double nu;
+    const double *frames;
+    double *out;
+    int64_t n;
+};
+
+__global__ void __launch_bounds__(128, 6) frame_coefficients_kernel(const __grid_constant__ FrameParams P) {
+    __shared__ TableSmem T;
+    load_table(T, P.M);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = warp; i < P.n; i += warps) {
+        const double *f = P.frames + 5 * i;
+        double out[11];
+        coefficients(T, P.M, f[0], f[1], f[2], f[3], f[4], P.nu, out);
+        if (lane < 11) {
+            double v = 0.0;
+#pragma unroll
+            for (int k = 0; k < 11; ++k) v = k == lane ? out[k] : v;
+            P.out[11 * i + lane] = v;
+        }
+    }
+}
+
 namespace {
 
 // ------------------------------------------------------------ host tables
@@ -255,5 +290,29 @@ extern "C" int bhn_brick_precompute(const double *rho, const double *theta_e, co
     const int64_t blocks = std::min<int64_t>((cells + 3) / 4, (int64_t)sms * 16);
     precompute_kernel<<<(unsigned)blocks, 128, 0, as_stream(stream)>>>(P);
     BHN_LAUNCH_CHECK("precompute_kernel");
+    return BHN_OK;
+}
+
+extern "C" int bhn_synchrotron_coefficients(const double *frames, int64_t n, const bhn_synchrotron_model *m,
+                                            double *out, void *stream) {
+    using namespace bhn;
+    using namespace bhn::synch;
+    if (n < 1) return fail(BHN_ERR_VALUE, "at least one plasma frame is required");
+    if (!frames || !out) return fail(BHN_ERR_VALUE, "missing frame or output buffer");
+    static FrameParams P;  // ~10 KB: kept off the host stack; filled under the lock
+    static std::mutex lock;
+    std::lock_guard<std::mutex> g(lock);
+    int rc = fill_model(m, P.M);
+    if (rc) return rc;
+    P.nu = m->nu_hz;
+    P.frames = frames;
+    P.out = out;
+    P.n = n;
+    int dev = 0, sms = 148;
+    BHN_CUDA_TRY(cudaGetDevice(&dev));
+    BHN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t blocks = std::min<int64_t>((n + 3) / 4, (int64_t)sms * 16);
+    frame_coefficients_kernel<<<(unsigned)blocks, 128, 0, as_stream(stream)>>>(P);
+    BHN_LAUNCH_CHECK("frame_coefficients_kernel");
     return BHN_OK;
 }

@@ -328,6 +328,48 @@ def precompute_fixtures(grmhd, calibration, cb, synchrotron) -> dict[str, np.nda
     return out
 
 
+def frame_fixtures(synchrotron) -> dict[str, np.ndarray]:
+    """ThermalSynchrotronCoefficients / NonthermalPowerLawSynchrotronCoefficients /
+    HybridSynchrotronCoefficients.coefficients(frame, nu_hz)
+    (synchrotron.py:248, 290, 318) on seeded local plasma frames (density,
+    temperature, field and pitch spread over the renderer's ranges, plus edge
+    frames: no density, no field, a tiny and a zero temperature, field along and
+    across the line of sight), four model settings and two frequencies."""
+    rng = np.random.default_rng(20261204)
+    n = 48
+    frames = np.stack([10.0 ** rng.uniform(2, 8, n), 10.0 ** rng.uniform(-1.5, 2.5, n), 10.0 ** rng.uniform(-1, 3, n),
+                       rng.uniform(-1, 1, n), rng.uniform(-math.pi, math.pi, n)], axis=1)
+    edge = np.array([[0.0, 10.0, 30.0, 0.3, 0.1], [1e6, 10.0, 0.0, 0.3, 0.1], [1e6, 1e-10, 30.0, 0.0, 0.0],
+                     [1e6, 0.0, 30.0, 0.5, 1.0], [1e6, 20.0, 30.0, 1.0, -2.0], [1e6, 20.0, 30.0, -1.0, 2.0],
+                     [1e6, 20.0, 30.0, 0.0, math.pi / 2], [3e5, 150.0, 500.0, 0.9, -0.7]])
+    frames = np.concatenate([frames, edge])
+    models = {
+        "hybrid": synchrotron.HybridSynchrotronCoefficients(),
+        "thermal": synchrotron.ThermalSynchrotronCoefficients(gamma_grid_size=96, pitch_nodes=9,
+                                                             faraday_rotation_scale=0.7, faraday_conversion_scale=1.3),
+        "nonthermal": synchrotron.NonthermalPowerLawSynchrotronCoefficients(p=2.8, gamma_min=30.0, gamma_max=3e4,
+                                                                           nonthermal_fraction=0.1, gamma_grid_size=100,
+                                                                           pitch_nodes=12, absorption_scale=0.5,
+                                                                           faraday_scale=0.3),
+        "hybrid_custom": synchrotron.HybridSynchrotronCoefficients(
+            thermal=synchrotron.ThermalSynchrotronCoefficients(gamma_grid_size=64, pitch_nodes=8),
+            nonthermal=synchrotron.NonthermalPowerLawSynchrotronCoefficients(gamma_grid_size=300, pitch_nodes=20)),
+    }
+    out = {"frames": frames}
+    for name, model in models.items():
+        for nu in (230e9, 86e9):
+            t0 = time.time()
+            vals = []
+            for f in frames:
+                frame = synchrotron.LocalPlasmaFrame(*[float(x) for x in f])
+                c = model.coefficients(frame, nu)
+                vals.append([c.j_i, c.j_q, c.j_u, c.j_v, c.alpha_i, c.alpha_q, c.alpha_u, c.alpha_v, c.rho_v, c.rho_q,
+                             c.rho_u])
+            out[f"{name}_{int(nu / 1e9)}"] = np.array(vals)
+            print(f"  frames {name} nu={nu:.3g}: {time.time() - t0:.1f}s", flush=True)
+    return out
+
+
 def exact_step_fixtures(pt, synchrotron) -> dict[str, np.ndarray]:
     """polarized_transfer.stokes_step_exact (polarized_transfer.py:51-70) on
     seeded coefficient sets and step lengths, including pure emission, pure
@@ -498,7 +540,7 @@ def main() -> None:
     ap.add_argument("--reference", default=env_ref, required=env_ref is None,
                     help="the reference project's python/ directory (default: $BHN_REFERENCE_PYTHON)")
     ap.add_argument("--only", default="",
-                    help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb,accel,accelreg")
+                    help="comma list of micro,kerr,ray,precompute,exact,grrt,bricknpz,rgb,accel,accelreg,frames")
     args = ap.parse_args()
     sys.path.insert(0, args.reference)
     sys.path.insert(0, str(REPO / "blackhole-sim_b200"))
@@ -534,6 +576,9 @@ def main() -> None:
     if not only or "accel" in only:
         np.savez_compressed(HERE / "accel.npz", **accel_fixtures(cb, acc, kerr, pt, grmhd))
         print("wrote accel.npz")
+    if not only or "frames" in only:
+        np.savez_compressed(HERE / "synchrotron_frames.npz", **frame_fixtures(synchrotron))
+        print("wrote synchrotron_frames.npz")
     if not only or "accelreg" in only:
         np.savez_compressed(HERE / "accel_regression.npz",
                             **accel_regression_fixtures(grmhd, calibration, cb, acc, pr, physics))
