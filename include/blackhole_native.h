@@ -243,19 +243,24 @@ int bhn_render_launch(const void *records, const void *tables, int32_t nr, int32
                       int64_t scratch_bytes, bhn_render_stats *stats, void *stream);
 
 /* bhn_render_prepare + bhn_render_launch for callers that cannot allocate
- * device memory (no counterpart in the reference).  Code that runs while a
- * stream is being captured into a CUDA graph may not call cudaMalloc, and some
- * hosts own all device memory through their own allocator; such callers pass
- * only inputs and outputs.  The scratch is a fixed 64 KiB array in the
- * library's device image (held by every GPU that loads the library until the
- * process exits), so at most BHN_NOALLOC_MAX_VIEWS views fit in one call; more
- * is rejected with BHN_ERR_VALUE.  The first call on a device looks up that
- * array's device address (cudaGetSymbolAddress) with the device current, so
- * make the first call on each device before any stream capture.  All calls on
- * a device share the array: calls that overlap on the GPU (different streams,
+ * device memory (no counterpart in the reference).  Some hosts own all device
+ * memory through their own allocator or a pool sized at start-up, and a
+ * library they load may not allocate beside it; real-time loops may not take
+ * the device-wide synchronisation that cudaMalloc / cudaFree can imply.  Such
+ * callers pass only inputs and outputs.  The scratch is a fixed 64 KiB array
+ * in the library's device image (held by every GPU that loads the library
+ * until the process exits), so at most BHN_NOALLOC_MAX_VIEWS views fit in one
+ * call; more is rejected with BHN_ERR_VALUE.  The first call on a device does
+ * the set-up: it looks up that array's device address (cudaGetSymbolAddress)
+ * with the device current and keeps it for the process, so make the first
+ * call on each device before any stream capture, and do not call it after
+ * cudaDeviceReset.  All calls on a device share the array and each call
+ * rewrites the part it uses (the work-queue head and the launch totals are
+ * zeroed by every launch): calls that overlap on the GPU (different streams,
  * or the same stream from several host threads without ordering) race.  The
- * function allocates nothing (no cudaMalloc / cudaFree); h_views is host
- * memory copied before return; stats may be NULL. */
+ * function allocates nothing (no cudaMalloc / cudaFree, no library allocator);
+ * h_views is ordinary host memory, copied into the array before the call
+ * returns; stats may be NULL. */
 #define BHN_NOALLOC_MAX_VIEWS 120
 int bhn_render_noalloc(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np,
                        const bhn_view *h_views, int32_t n_views, const bhn_render_config *cfg, void *out,
@@ -308,7 +313,7 @@ int bhn_mlp_adam(float *params, float *grad, float *m, float *v, float lr, float
 /* The inference path on given standardised feature rows (n x 8) -> n outputs. */
 int bhn_mlp_infer(const void *blob, const float *features, int64_t n, float *out, void *stream);
 /* Step-doubling controller over prepared views (bhn_render_prepare): float4
- * Stokes out, optional per-ray steps/status, samples appended while
+ * Stokes out, optional per-ray steps/status/Hamiltonian drift, samples appended while
  * *sample_count < capacity; counters[0..2] += RK2 stage pairs, accepted steps,
  * rejected attempts. */
 int bhn_adaptive_launch(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np, int32_t n_views,
@@ -316,8 +321,9 @@ int bhn_adaptive_launch(const void *records, const void *tables, int32_t nr, int
                         int64_t scratch_bytes, const bhn_adapt_params *params, float *samples,
                         unsigned long long *sample_count, unsigned long long sample_capacity,
                         unsigned long long *counters, void *stream);
-/* The learned-step ray loop over prepared views; counters[0..3] += RHS
- * evaluations, steps, fallbacks to the plain step, network evaluations. */
+/* The learned-step ray loop over prepared views (optional per-ray
+ * steps/status/Hamiltonian drift); counters[0..3] += RHS evaluations, steps,
+ * fallbacks, network evaluations. */
 int bhn_learned_launch(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np, int32_t n_views,
                        const bhn_render_config *cfg, void *out, const bhn_ray_outputs *ray_out, void *scratch,
                        int64_t scratch_bytes, const bhn_adapt_params *params, const void *blob,
@@ -348,6 +354,18 @@ typedef struct bhn_synchrotron_model {
  * 2..4096 nodes, pitch averages 1..64. */
 int bhn_brick_precompute(const double *rho, const double *theta_e, const double *b_con, int64_t cells,
                          const bhn_synchrotron_model *model, void *coeffs, int32_t coeff_bytes, void *stream);
+
+/* The model's 11 coefficients for n local plasma frames, FP64 on the device.
+ * Replaces ThermalSynchrotronCoefficients.coefficients,
+ * NonthermalPowerLawSynchrotronCoefficients.coefficients and
+ * HybridSynchrotronCoefficients.coefficients (python/blackhole_sim/
+ * synchrotron.py:248, 290, 318), per frame of synchrotron.py:28-44:
+ * frames[n][5] = (n_e_cm3, theta_e, b_gauss, cos_pitch_to_los, evpa_rad)
+ * (device), out[n][11] in PolarizedCoefficients field order, which is
+ * COEFF_NAMES order (device).  No nan_to_num, no Theta_e floor beyond the
+ * models' own; the scaling fields of the model are not used. */
+int bhn_synchrotron_coefficients(const double *frames, int64_t n, const bhn_synchrotron_model *model, double *out,
+                                 void *stream);
 
 /* ---- physical polarized GRRT through a GRMHD snapshot --------------------------
  * Replaces polarized_renderer.render_stokes_image (python/blackhole_sim/
