@@ -66,6 +66,7 @@ class AdaptStruct(ctypes.Structure):
         ("max_attempts", ctypes.c_int32),
         ("fallback", ctypes.c_int32),
         ("seed", ctypes.c_uint32),
+        ("substeps", ctypes.c_int32),
     ]
 
 
@@ -91,6 +92,7 @@ class AdaptConfig:
     max_attempts: int = 16
     fallback: str = "controller"   # learned: "plain" or "controller" takes a step that fails the check
     seed: int = 1
+    substeps: int = 1              # learned: RK2 steps of h / substeps per brick segment (1 or 2)
 
     def to_struct(self) -> AdaptStruct:
         if self.fallback not in FALLBACKS:
@@ -102,6 +104,9 @@ class AdaptConfig:
                                                              float(self.brick_scale), float(self.min_scale))
         s.interval, s.max_attempts, s.fallback = int(self.interval), int(self.max_attempts), FALLBACKS[self.fallback]
         s.seed = int(self.seed) & 0xFFFFFFFF
+        if self.substeps not in (1, 2):
+            raise ValueError("substeps must be 1 or 2")
+        s.substeps = int(self.substeps)
         return s
 
 

@@ -350,6 +350,7 @@ struct AdaptParams {
     int max_attempts;   // adaptive: attempts per step before forcing acceptance
     int fallback;       // learned: a failed check takes the plain step (0) or the controller's (1)
     uint32_t seed;
+    int substeps;       // learned: RK2 steps of h / substeps per brick segment (1 or 2)
 };
 
 // k1 at g and k2 at the Euler half step (the two stages of the RK2 midpoint step).
@@ -826,34 +827,50 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
                 alive = false;
                 continue;
             }
-            rk2_stages(g, h, C, pt, pphi, k1, k2, false);
-            n_eval += 2;
-            float e = 0.0f;
-            if (L.A.check_tol > 0.0f) {
-                // the Euler and midpoint solutions differ by h (k2 - k1).  The phi
-                // difference is weighted by sin(theta) (the angle it subtends):
-                // phi is cyclic, so its error does not feed back into the motion,
-                // and near the spin axis its coordinate rate ~ 1/sin^2(theta)
-                // would otherwise fail every proposal there.
-                const float sth = fabsf(__sinf(g.th_h));
-                e = mixed_norm(h * (k2.r - k1.r), h * (k2.th - k1.th), sth * h * (k2.ph - k1.ph), h * (k2.pr - k1.pr),
-                               h * (k2.pth - k1.pth), g, L.A.check_tol);
-            }
+            // the Euler and midpoint solutions of an RK2 step differ by h (k2 - k1).
+            // The phi difference is weighted by sin(theta) (the angle it subtends):
+            // phi is cyclic, so its error does not feed back into the motion, and
+            // near the spin axis its coordinate rate ~ 1/sin^2(theta) would
+            // otherwise fail every proposal there.
+            auto check = [&](const Geo &s0, float hs, const Deriv32 &a1, const Deriv32 &a2) -> float {
+                if (!(L.A.check_tol > 0.0f)) return 0.0f;
+                const float sth = fabsf(__sinf(s0.th_h));
+                return mixed_norm(hs * (a2.r - a1.r), hs * (a2.th - a1.th), sth * hs * (a2.ph - a1.ph),
+                                  hs * (a2.pr - a1.pr), hs * (a2.pth - a1.pth), s0, L.A.check_tol);
+            };
             Geo y;
-            if (!(e > 1.0f)) {
-                y = geo_advance(g, h, k2);
-            } else if (L.A.fallback == 0) {  // misprediction: the plain step
-                ++n_fb;
-                ++n_eval;
-                h = h_plain;
+            float e;
+            if (L.A.substeps == 2) {
+                // two RK2 steps of h / 2 and one brick segment over both: the form of
+                // the controller's accepted solution, without its full-h comparison step
+                const float hh = 0.5f * h;
+                rk2_stages(g, hh, C, pt, pphi, k1, k2, false);
+                e = check(g, hh, k1, k2);
+                const Geo ym = geo_advance(g, hh, k2);
+                Deriv32 k1b, k2b;
+                rk2_stages(ym, hh, C, pt, pphi, k1b, k2b, true);
+                e = fmaxf(e, check(ym, hh, k1b, k2b));
+                n_eval += 4;
+                if (!(e > 1.0f)) y = geo_advance(ym, hh, k2b);
+            } else {
                 rk2_stages(g, h, C, pt, pphi, k1, k2, false);
-                y = geo_advance(g, h, k2);
-            } else {  // misprediction: the step-doubling controller takes this step
+                n_eval += 2;
+                e = check(g, h, k1, k2);
+                if (!(e > 1.0f)) y = geo_advance(g, h, k2);
+            }
+            if (e > 1.0f) {
                 ++n_fb;
-                h = fmaxf(h * fmaxf(0.1f, 0.9f * rsqrtf(e)), L.A.h_floor);
-                float err;
-                unsigned long long n_rej = 0;
-                y = doubling_step(g, h, k1, C, pt, pphi, L.A, err, n_eval, n_rej);
+                if (L.A.fallback == 0) {  // misprediction: the plain step
+                    ++n_eval;
+                    h = h_plain;
+                    rk2_stages(g, h, C, pt, pphi, k1, k2, false);
+                    y = geo_advance(g, h, k2);
+                } else {  // misprediction: the step-doubling controller takes this step
+                    h = fmaxf(h * fmaxf(0.1f, 0.9f * rsqrtf(e)), L.A.h_floor);
+                    float err;
+                    unsigned long long n_rej = 0;
+                    y = doubling_step(g, h, k1, C, pt, pphi, L.A, err, n_eval, n_rej);
+                }
             }
             const float dr = (y.rh - g.rh) + (y.rl - g.rl), dph = (y.ph_h - g.ph_h) + (y.ph_l - g.ph_l);
             const float dph_u = dph > 3.14159f ? dph - kTwoPiH : (dph < -3.14159f ? dph + kTwoPiH : dph);
@@ -894,9 +911,9 @@ static int learn_params(const void *records, const void *tables, int32_t nr, int
     if (!ap) return fail(BHN_ERR_VALUE, "adapt params must not be NULL");
     if (!(ap->tol > 0.0f) || !(ap->h_floor > 0.0f) || !(ap->h_ceil >= ap->h_floor) || ap->interval < 1 ||
         ap->max_attempts < 1 || (ap->fallback != 0 && ap->fallback != 1) || !(ap->sample_prob >= 0.0f) ||
-        !(ap->check_tol >= 0.0f) || !(ap->min_scale > 0.0f))
+        !(ap->check_tol >= 0.0f) || !(ap->min_scale > 0.0f) || (ap->substeps != 1 && ap->substeps != 2))
         return fail(BHN_ERR_VALUE, "adapt params: need tol > 0, 0 < h_floor <= h_ceil, check_tol >= 0, min_scale > 0, "
-                                   "max_attempts >= 1");
+                                   "max_attempts >= 1, substeps 1 or 2");
     if (n_views < 1 || !records || !tables || !out || !scratch) return fail(BHN_ERR_VALUE, "missing buffers or views");
     ScratchLayout SL = scratch_layout(n_views);
     if (scratch_bytes < SL.total) return fail(BHN_ERR_VALUE, "scratch buffer is smaller than bhn_render_scratch_bytes()");
@@ -938,6 +955,7 @@ static int learn_params(const void *records, const void *tables, int32_t nr, int
     L.A.interval = ap->interval;
     L.A.max_attempts = ap->max_attempts;
     L.A.seed = ap->seed;
+    L.A.substeps = ap->substeps;
     BHN_CUDA_TRY(cudaMemsetAsync(&P.q->next, 0, sizeof(unsigned long long), s));
     return BHN_OK;
 }

@@ -289,6 +289,9 @@ typedef struct bhn_adapt_params {
     int32_t max_attempts; /* controller: attempts per step before the step is forced */
     int32_t fallback;    /* learned: a step failing the check is the plain step (0) or the controller's (1) */
     uint32_t seed;       /* controller: sample-selection hash seed */
+    int32_t substeps;    /* learned: 1 = one RK2 step of the proposed h per brick segment; 2 = two RK2 steps of
+                            h / 2 per segment (the controller's accepted-solution form, without its h-step
+                            error estimate), each half step checked */
 } bhn_adapt_params;
 
 /* Sample rows: 8 raw features (log r, cos theta, asinh p_r, asinh p_theta, a,
