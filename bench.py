@@ -529,13 +529,15 @@ def bench_views(args) -> dict | None:
         h_drift = studies._drift_summary(rr.h_drift.cpu().numpy().astype(np.float64), rr.status.cpu().numpy())
         del rr
         if not args.no_accuracy:
-            # Stokes error against the FP64 kernel at h/4 on centred crops (at most 128^2) of four views
+            # Stokes error against the FP64 kernel at h/4 on a crop through the torus
+            # image (right of the shadow, at most 128^2: the image workload's crop) of four views
             db64 = bn.DeviceBrick(scenes.shared_brick(), device=device, precisions=("fp32", "fp64"))
             per = []
             for v in views[:4]:
-                w, h = min(v.width, 128), min(v.height, 128)
-                crop = ((v.width - w) // 2, (v.height - h) // 2, w, h)
-                per.append(studies.fine_step_check(db64, v, crop, config=cfg))
+                w, h = min(max(v.width // 4, 16), 128), min(max(v.height // 4, 16), 128)
+                x0 = min(v.width // 2 + v.width * 3 // 32, v.width - w)
+                y0 = max(v.height // 2 - v.height // 8, 0)
+                per.append(studies.fine_step_check(db64, v, (x0, y0, w, h), config=cfg))
             keys = ("rel_l1_I", "rel_l1_Q", "rel_l1_U", "rel_l1_V", "flux_weighted_dm")
             accuracy = {"views": [{"side": [v.width, v.height], "spin_a": v.spin_a, "inclination_deg": v.inclination_deg,
                                    "crop": a["crop"], "mask_fraction": a["mask_fraction"]["fine_step"],
@@ -1277,10 +1279,9 @@ def time_to_image(device, side: int, reps: int, spin: float = 0.9375, incl: floa
     plain_key = min((k for k in ok if k.startswith("plain")), key=lambda k: ok[k], default=None)
     # Hamiltonian drift of the learned loop's rays: one more launch with per-ray outputs
     lr = learned.render_learned(db, [v], net, learned.AdaptConfig(), repeats=1, ray_outputs=True)
-    h_drift = None
-    if lr.rnd.h_drift is not None:
-        h_drift = studies._drift_summary(lr.rnd.result().per_ray("h_drift").cpu().numpy().astype(np.float64),
-                                         lr.rnd.result().per_ray("status").cpu().numpy())
+    res = lr.renderer.result()
+    h_drift = studies._drift_summary(res.per_ray("h_drift").cpu().numpy().astype(np.float64),
+                                     res.per_ray("status").cpu().numpy())
     out = {"workload": f"{side}x{side} rays, a={spin}, i={incl}deg, horizon guard, 256x128x256x11 float32 torus "
                        "brick (seed 1), reference FP64 kernel at h/16",
            "mask_fraction": float(mask.mean()), "timing": f"each method: the fastest of {reps} launches (CUDA events)",

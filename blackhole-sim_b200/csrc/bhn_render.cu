@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -294,6 +295,12 @@ __device__ __forceinline__ PixelRef ordered_pixel(const ViewDev *views, const in
     return pixel_in_columns(v, k - left, v.axis_x1, v.crop_w - v.axis_x1, tw, th);
 }
 
+// v clamped into FP32's finite range (NaN stays NaN).
+__device__ __forceinline__ double sat_double(double v) {
+    return isnan(v) ? v : fmax(fmin(v, (double)FLT_MAX), -(double)FLT_MAX);
+}
+__device__ __forceinline__ float sat_float(double v) { return (float)sat_double(v); }
+
 // v as an unevaluated float pair hi + lo (hi = v rounded, lo = the remainder).
 __device__ __forceinline__ void split(double v, float &hi, float &lo) {
     hi = (float)v;
@@ -306,7 +313,8 @@ constexpr double kNearHorizon = 0.1;  // FP64 island: steps that start within 0.
 // p_theta' ~ p_phi^2 cos / sin^3 throws p_theta to ~1e21; the FP64 method
 // carries such a ray on (its squares ~1e42 stay finite), FP32's would overflow
 // and end the ray as invalid.  Steps that start within 1e-4 rad of a pole or
-// with |p_r| or |p_theta| >= 1e15 therefore run in FP64.
+// with |p_r| or |p_theta| >= 1e15 therefore run in FP64, and so does any step
+// whose FP32 result overflows.
 constexpr float kPoleIsland = 1.0e-4f;
 constexpr float kMomentumIsland = 1.0e15f;
 
@@ -381,30 +389,37 @@ constexpr float kEpsF = 1.0e-7f;
 constexpr float kTmaxH = (float)(kPi - kEpsTheta);  // pi - eps as a float pair (kerr.py:35-36 upper clamp)
 constexpr float kTmaxL = (float)((kPi - kEpsTheta) - (double)kTmaxH);
 
-// sin and cos on [0, pi/2] by their Taylor series (through x^11 and x^12; the
-// truncation error is below 6e-8 at pi/2), evaluated by Horner in x^2.
+// sin and cos on [eps, pi/2].  Below x = 1/4 (next to a pole, where the
+// metric inverse g^phiphi ~ 1/sin^2 needs sin to full relative precision):
+// the Taylor series through x^7 and x^8 (truncation below 1.2e-11 relative),
+// by Horner in x^2.  Above it the hardware __sincosf (absolute error about
+// 2^-21.4, relative below 1.5e-6 there), at a fraction of the series' cost.
 __device__ __forceinline__ void sincos_quadrant(float x, float &s, float &c) {
-    const float u = x * x;
-    float ps = fmaf(u, -2.5052108385e-8f, 2.7557319224e-6f);  // -1/11!, 1/9!
-    ps = fmaf(u, ps, -1.9841269841e-4f);                        // -1/7!
-    ps = fmaf(u, ps, 8.3333333333e-3f);                         // 1/5!
-    ps = fmaf(u, ps, -1.6666666667e-1f);                        // -1/3!
-    s = fmaf(x * u, ps, x);
-    float pc = fmaf(u, 2.0876756988e-9f, -2.7557319224e-7f);    // 1/12!, -1/10!
-    pc = fmaf(u, pc, 2.4801587302e-5f);                         // 1/8!
-    pc = fmaf(u, pc, -1.3888888889e-3f);                        // -1/6!
-    pc = fmaf(u, pc, 4.1666666667e-2f);                         // 1/4!
-    pc = fmaf(u, pc, -0.5f);                                    // -1/2!
-    c = fmaf(u, pc, 1.0f);
+    if (x < 0.25f) {
+        const float u = x * x;
+        float ps = fmaf(u, -1.9841269841e-4f, 8.3333333333e-3f);  // -1/7!, 1/5!
+        ps = fmaf(u, ps, -1.6666666667e-1f);                        // -1/3!
+        s = fmaf(x * u, ps, x);
+        float pc = fmaf(u, 2.4801587302e-5f, -1.3888888889e-3f);   // 1/8!, -1/6!
+        pc = fmaf(u, pc, 4.1666666667e-2f);                         // 1/4!
+        pc = fmaf(u, pc, -0.5f);                                    // -1/2!
+        c = fmaf(u, pc, 1.0f);
+    } else {
+        __sincosf(x, &s, &c);
+    }
 }
 
 // sin(theta), cos(theta) from d, the distance of theta from the pole nearer
 // at the step start (south: theta = pi - d).  d keeps full relative precision
 // next to either pole because it is formed from the compensated theta, which
-// is what the near-pole metric inverse (g^phiphi ~ 1/sin^2) needs.
+// is what the near-pole metric inverse (g^phiphi ~ 1/sin^2) needs.  A
+// midpoint may lie past the equator (d > pi/2: x is the distance to the other
+// pole) or past the other pole altogether (d > pi - eps, even by many radians
+// when p_theta is large): kerr.py:35-36 clips theta into [eps, pi - eps], which
+// here is x >= eps, so x never leaves [eps, pi/2] where the series holds.
 __device__ __forceinline__ void sincos_pole(float d, bool south, float &s, float &c) {
     const bool over = d > kHalfPiF;  // a half step may cross the equator
-    const float x = over ? (kPiH - d) + kPiL : d;
+    const float x = fmaxf(over ? (kPiH - d) + kPiL : d, kEpsF);
     sincos_quadrant(x, s, c);
     c = (over != south) ? -c : c;
     s = fmaxf(s, kEpsF);  // sin^2 >= eps^2 (kerr.py:93)
@@ -432,13 +447,17 @@ struct Deriv32 {
 };
 
 // Hamiltonian equations of kerr.py:285-303 written through
-//   2 Sigma H = Delta p_r^2 + p_theta^2 + P^2 - W^2 / Delta,
+//   2 Sigma H = F = Delta p_r^2 + p_theta^2 + P^2 - W^2 / Delta,
 //   P = p_phi / sin + a sin p_t,  W = (r^2 + a^2) p_t + a p_phi,
 // which is g^{mu nu} p_mu p_nu of kerr.py:86-102 regrouped; x' = dH/dp and
 // p' = -dH/dx are its exact derivatives (the quotient-rule sums of
-// kerr.py:236-282 collapse to these few terms).  Delta is formed as
-// (r - r+)(r - r-) from the compensated horizon distance x = r - r+, since
-// r^2 - 2r + a^2 cancels to nothing in FP32 next to the horizon.
+// kerr.py:236-282 collapse to these few terms).  With Q = W / Delta and
+// G = F / Sigma (= 2H):
+//   p_r'     = [(1 - r)(p_r^2 + Q^2) + r (2 p_t Q + G)] / Sigma,
+//   p_theta' = cos [P (p_phi / sin^2 - a p_t) - G a^2 sin] / Sigma.
+// Delta is formed as (r - r+)(r - r-) from the compensated horizon distance
+// x = r - r+, since r^2 - 2r + a^2 cancels to nothing in FP32 next to the
+// horizon.
 __device__ __forceinline__ void rhs32(float r, float x, float s, float c, float pr, float pth, float pt, float pphi,
                                       float a, float a2, float dpm, Deriv32 &d) {
     const float r2 = r * r;
@@ -448,17 +467,17 @@ __device__ __forceinline__ void rhs32(float r, float x, float s, float c, float 
     const float iD = 1.0f / D;
     const float is = 1.0f / s;
     const float W = fmaf(r2 + a2, pt, a * pphi);
-    const float P = fmaf(a * s, pt, pphi * is);
+    const float P = fmaf(a * pt, s, pphi * is);
     const float Q = W * iD;
-    const float F = fmaf(D * pr, pr, fmaf(pth, pth, fmaf(P, P, -W * Q)));
-    d.r = D * pr * iS;
+    const float Dpr = D * pr;
+    const float F = fmaf(Dpr, pr, fmaf(pth, pth, fmaf(P, P, -W * Q)));
+    const float G = F * iS;
+    d.r = Dpr * iS;
     d.th = pth * iS;
     d.ph = fmaf(P, is, -a * Q) * iS;
-    const float dFr = fmaf(2.0f * r - 2.0f, fmaf(pr, pr, Q * Q), -4.0f * r * pt * Q);
-    d.pr = fmaf(-0.5f, dFr, F * r * iS) * iS;
-    const float dFth = 2.0f * P * c * fmaf(a, pt, -pphi * is * is);
-    d.pth = fmaf(-0.5f, dFth, -F * a2 * s * c * iS) * iS;
-    d.H = 0.5f * F * iS;
+    d.pr = fmaf(1.0f - r, fmaf(pr, pr, Q * Q), r * fmaf(pt + pt, Q, G)) * iS;
+    d.pth = c * fmaf(P, fmaf(pphi * is, is, -a * pt), -G * (a2 * s)) * iS;
+    d.H = 0.5f * G;
 }
 
 // rhs32's Hamiltonian form in FP64 (the near-horizon island of the FP32 kernel).
@@ -518,7 +537,9 @@ struct Tracer32 {
     // p_r ~ 1/Delta leaves FP32's exponent range there.
     // Returns 0 (finite), 1 (non-finite) or 2 (horizon guard: the midpoint lies
     // inside the horizon; the state is left unchanged).
-    __device__ __forceinline__ int step_fp64(const ViewDev &v, bool guard, float &dr, float &dph) {
+    // Not inlined: the FP64 step runs for a few steps in a thousand, and keeping
+    // its code out of the FP32 loop keeps that loop's registers for itself.
+    __device__ __noinline__ int step_fp64(const ViewDev &v, bool guard, float &dr, float &dph) {
         const double r = (double)rh + (double)rl;
         const double th = (double)th_h + (double)th_l;
         const double ph = (double)ph_h + (double)ph_l;
@@ -532,13 +553,17 @@ struct Tracer32 {
                v.r_minus, k2);
         const double rn = r + h * k2.r, thn = safe_theta(th + h * k2.th), phn = ph + h * k2.ph;
         const double prn = pr + h * k2.pr, pthn = pth + h * k2.pth;
-        dr = (float)(rn - r);
-        dph = (float)(phn - ph);
-        split(rn, rh, rl);
+        // a catastrophic step of the reference's method (a ray flung off the pole
+        // or out of the horizon) can leave FP32's range while FP64 stays finite:
+        // such values are kept saturated at +-FLT_MAX, which ends the ray with
+        // the FP64 method's status (captured at r -> -inf, escaped at r -> +inf)
+        dr = sat_float(rn - r);
+        dph = sat_float(phn - ph);
+        split(sat_double(rn), rh, rl);
         split(thn, th_h, th_l);
-        split(phn, ph_h, ph_l);
-        pr = (float)prn;
-        pth = (float)pthn;
+        split(sat_double(phn), ph_h, ph_l);
+        pr = sat_float(prn);
+        pth = sat_float(pthn);
         return (isfinite(rn) && isfinite(thn) && isfinite(phn) && isfinite(prn) && isfinite(pthn)) ? 0 : 1;
     }
 
@@ -548,15 +573,12 @@ struct Tracer32 {
                                         int nt, int np, const ViewDev *__restrict__ views) {
         if (rh < C.r_guard && pr < 0.0f) return BHN_RAY_CAPTURED;  // horizon guard (flag; off by default)
         const float r0 = rh + rl, th0 = th_h + th_l, ph0 = ph_h + ph_l;
-        float dr, dph;
-        bool finite;
+        float dr = 0.0f, dph = 0.0f;
+        bool finite = true;
         const bool south = th_h > kHalfPiF;
         const float d0 = south ? (kPiH - th_h) + (kPiL - th_l) : th0;
-        if (rh < C.r_near || d0 < kPoleIsland || !(fabsf(pth) < kMomentumIsland && fabsf(pr) < kMomentumIsland)) {
-            const int rc = step_fp64(views[vi], C.r_guard > 0.0f, dr, dph);
-            if (rc == 2) return BHN_RAY_CAPTURED;
-            finite = rc == 0;
-        } else {
+        bool fp64 = rh < C.r_near || d0 < kPoleIsland || !(fabsf(pth) < kMomentumIsland && fabsf(pr) < kMomentumIsland);
+        if (!fp64) {
             float s, c;
             sincos_pole(d0, south, s, c);
             const float x0 = (rh - C.rp_h) + (rl - C.rp_l);
@@ -576,20 +598,31 @@ struct Tracer32 {
             dr = h * k2.r;
             const float dth = h * k2.th;
             dph = h * k2.ph;
-            kahan_add(rh, rl, dr);
-            kahan_add(th_h, th_l, dth);
-            kahan_add(ph_h, ph_l, dph);
-            pr = fmaf(h, k2.pr, pr);
-            pth = fmaf(h, k2.pth, pth);
-            finite = isfinite(dr + dth + dph + pr + pth);
-            // theta clamp (kerr.py:312)
-            if (th_h + th_l < kEpsF) {
-                th_h = kEpsF;
-                th_l = 0.0f;
-            } else if ((th_h - kTmaxH) + (th_l - kTmaxL) > 0.0f) {
-                th_h = kTmaxH;
-                th_l = kTmaxL;
+            const float prn = fmaf(h, k2.pr, pr), pthn = fmaf(h, k2.pth, pth);
+            // An FP32 overflow here (a ray flung off the pole or out of the
+            // horizon reaches momenta of 1e30 and more, whose squares FP64 still
+            // holds) sends the step to FP64, from the untouched start state.
+            fp64 = !isfinite(dr + dth + dph + prn + pthn);
+            if (!fp64) {
+                kahan_add(rh, rl, dr);
+                kahan_add(th_h, th_l, dth);
+                kahan_add(ph_h, ph_l, dph);
+                pr = prn;
+                pth = pthn;
+                // theta clamp (kerr.py:312)
+                if (th_h + th_l < kEpsF) {
+                    th_h = kEpsF;
+                    th_l = 0.0f;
+                } else if ((th_h - kTmaxH) + (th_l - kTmaxL) > 0.0f) {
+                    th_h = kTmaxH;
+                    th_l = kTmaxL;
+                }
             }
+        }
+        if (fp64) {
+            const int rc = step_fp64(views[vi], C.r_guard > 0.0f, dr, dph);
+            if (rc == 2) return BHN_RAY_CAPTURED;
+            finite = rc == 0;
         }
         ++steps;
         const float th1 = th_h + th_l;
@@ -625,16 +658,17 @@ struct Tracer32 {
                     const float wt = (tmid - T.gtf[it]) * T.idt[it];
                     const float wp = (pw - T.gpf[ip]) * T.idp[ip];
                     const float owr = 1.0f - wr, owt = 1.0f - wt, owp = 1.0f - wp;
-                    const int64_t c00 = ((int64_t)ir * nt + it) * np;
-                    const int64_t cells[4] = {c00, c00 + np, c00 + (int64_t)nt * np, c00 + (int64_t)nt * np + np};
+                    // 32-bit cell offsets (launch_render admits bricks of < 2^32 float4 records)
+                    const uint32_t c00 = ((uint32_t)ir * nt + it) * np;
+                    const uint32_t cells[4] = {c00, c00 + np, c00 + (uint32_t)(nt * np), c00 + (uint32_t)(nt * np + np)};
                     const float wrt[4] = {owr * owt, owr * wt, wr * owt, wr * wt};
                     // channels in pairs on the paired FP32 FMA (each lane one fmaf, same order)
                     float2 c01 = make_float2(0.0f, 0.0f), c23 = c01, c45 = c01, c67 = c01, c89 = c01;
                     float c10 = 0.0f;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const float4 *p0 = rec + 3 * (cells[q] + ip);
-                        const float4 *p1 = rec + 3 * (cells[q] + ip1);
+                        const float4 *p0 = rec + 3u * (cells[q] + (uint32_t)ip);
+                        const float4 *p1 = rec + 3u * (cells[q] + (uint32_t)ip1);
                         const float w0 = wrt[q] * owp, w1 = wrt[q] * wp;
                         const float2 W0 = make_float2(w0, w0), W1 = make_float2(w1, w1);
                         const float4 a0 = __ldg(p0), b0 = __ldg(p0 + 1), c0 = __ldg(p0 + 2);
@@ -682,15 +716,26 @@ struct Tracer32 {
         return -1;
     }
 
-    __device__ __forceinline__ void finish(void *out, int status, const StepConst &C, const ViewDev *) {
+    __device__ __forceinline__ void finish(void *out, int status, const StepConst &C, const ViewDev *views) {
         if (status != BHN_RAY_INVALID) {  // drift at the final state (kerr.py:360, 367)
             const bool south = th_h > kHalfPiF;
             const float d0 = south ? (kPiH - th_h) + (kPiL - th_l) : th_h + th_l;
-            float s, c;
-            sincos_pole(d0, south, s, c);
-            Deriv32 k;
-            rhs32(rh + rl, (rh - C.rp_h) + (rl - C.rp_l), s, c, pr, pth, pt, pphi, C.a, C.a2, C.dpm, k);
-            drift = fmaxf(drift, fabsf(fabsf(k.H) - H0));
+            if (rh < C.r_near || d0 < kPoleIsland ||
+                !(fabsf(pth) < kMomentumIsland && fabsf(pr) < kMomentumIsland && fabsf(rh) < kMomentumIsland)) {
+                // a state the FP32 right-hand side cannot evaluate (the islands, or a
+                // ray flung to |r| >= 1e15 by its last step): H in FP64
+                const ViewDev &v = views[vi];
+                Deriv64 k;
+                rhs64h((double)rh + (double)rl, (double)th_h + (double)th_l, pr, pth, pt, pphi, v.a, v.r_plus,
+                       v.r_minus, k);
+                drift = fmaxf(drift, (float)fmin(fabs(fabs(k.H) - (double)H0), (double)FLT_MAX));
+            } else {
+                float s, c;
+                sincos_pole(d0, south, s, c);
+                Deriv32 k;
+                rhs32(rh + rl, (rh - C.rp_h) + (rl - C.rp_l), s, c, pr, pth, pt, pphi, C.a, C.a2, C.dpm, k);
+                drift = fmaxf(drift, fabsf(fabsf(k.H) - H0));
+            }
         }
         // np.nan_to_num(S, nan=0, posinf=0, neginf=0) (accelerated_renderer.py:126)
         float4 o;
@@ -701,7 +746,9 @@ struct Tracer32 {
         reinterpret_cast<float4 *>(out)[out_idx] = o;
     }
 
-    __device__ __forceinline__ float drift_f() const { return drift; }
+    // The drift output is a float: drifts beyond its range (a catastrophic last
+    // step can reach 1e60 in FP64) are stored as FLT_MAX.
+    __device__ __forceinline__ float drift_f() const { return fminf(drift, FLT_MAX); }
 
     static __device__ __forceinline__ void write_zero(void *out, int64_t idx) {
         reinterpret_cast<float4 *>(out)[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -843,7 +890,7 @@ struct Tracer64 {
         o[1] = make_double2((poison || !isfinite(S2)) ? 0.0 : S2, (poison || !isfinite(S3)) ? 0.0 : S3);
     }
 
-    __device__ __forceinline__ float drift_f() const { return (float)drift; }
+    __device__ __forceinline__ float drift_f() const { return (float)fmin(drift, (double)FLT_MAX); }
 
     static __device__ __forceinline__ void write_zero(void *out, int64_t idx) {
         double2 *o = reinterpret_cast<double2 *>(out) + 2 * idx;
@@ -1064,6 +1111,8 @@ static int launch_render(const void *records, const void *tables, int32_t nr, in
     if (n_views < 1) return fail(BHN_ERR_VALUE, "at least one view is required");
     if (!records || !tables || !out || !scratch) return fail(BHN_ERR_VALUE, "records, tables, out and scratch must not be NULL");
     if (nr < 2 || nt < 2 || np < 2) return fail(BHN_ERR_VALUE, "brick grids must contain at least 2 values");
+    if (cfg->precision == 0 && 3 * (int64_t)nr * nt * np >= ((int64_t)1 << 32))
+        return fail(BHN_ERR_VALUE, "the FP32 kernel takes bricks of fewer than 2^32 / 3 cells (32-bit record offsets)");
     ScratchLayout L = scratch_layout(n_views);
     if (scratch_bytes < L.total) return fail(BHN_ERR_VALUE, "scratch buffer is smaller than bhn_render_scratch_bytes()");
     if (reinterpret_cast<uintptr_t>(records) % 16 || reinterpret_cast<uintptr_t>(tables) % 16 ||

@@ -99,7 +99,7 @@ def test_scene_crop_parity(scene_brick):
     vg = bn.View(1024, 1024, max_steps=4096, crop=(480, 480, 64, 64), horizon_guard=True)
     g_img = _oracle(vg, b)[0]
     stable = np.all(g_img == o_img, axis=-1)
-    assert stable.mean() > 0.5
+    assert stable.mean() >= 0.56   # 0.562: the crop is the shadow's edge, where most captured rays overshoot
     assert rel_l1(img32[..., 0][stable], o_img[..., 0][stable]) <= FP32_I_REL_L1
     assert flux_weighted_dm(img32[stable], o_img[stable]) <= FP32_DM
     g32 = bn.render(db, vg, precision="fp32").image().cpu().numpy().astype(np.float64)
@@ -242,6 +242,42 @@ def test_full_image1024_properties(scene_brick):
     i32 = bn.render(db, vg, precision="fp32").image().cpu().numpy().astype(np.float64)
     assert rel_l1(i32[..., 0][cond], f64[..., 0][cond]) <= FP32_I_REL_L1
     assert flux_weighted_dm(i32[cond], f64[cond]) <= FP32_DM
+
+
+@pytest.mark.parametrize("name,spin,incl,side,steps,seed", [("c2", 0.9375, 17.0, 1024, 4096, 0),
+                                                              ("c3", 0.998, 60.0, 4096, 8192, 3)])
+def test_fp32_ends_rays_as_fp64_does(name, spin, incl, side, steps, seed):
+    """BASELINE configs 2 and 3 at full size, the reference's semantics
+    (horizon guard off): no ray ends non-finite in FP32 where the FP64 method
+    stays finite (FP32 steps that overflow are taken in FP64), no ray runs to
+    max_steps in FP32 alone (midpoints past a pole clip like kerr.py:35-36),
+    and the status counts agree to a few rays in 10^4 (statuses of the rays the
+    reference's own step flings off the pole or out of the horizon are chaotic
+    in the last bit)."""
+    b = bricks.torus_brick(256, 128, 256, spin_a=spin, seed=seed, dtype=np.float32)
+    db = bn.DeviceBrick(b, precisions=("fp32", "fp64"))
+    v = bn.View(side, side, spin_a=spin, inclination_deg=incl, max_steps=steps)
+    r32 = bn.render(db, v, precision="fp32", ray_outputs=True)
+    s32 = r32.per_ray("status").cpu().numpy()
+    s64 = bn.render(db, v, precision="fp64", ray_outputs=True).per_ray("status").cpu().numpy()
+    invalid, max_steps = 3, 0
+    assert int(np.sum((s32 == invalid) & (s64 != invalid))) == 0
+    assert int(np.sum((s32 == max_steps) & (s64 != max_steps))) == 0
+    assert int(np.sum(s32 == invalid)) == int(np.sum(s64 == invalid)) == 0
+    assert np.mean(s32 != s64) <= 1e-3
+    st = r32.stats()
+    assert np.isfinite(st.max_h_drift) and np.isfinite(st.max_h_drift_escaped)
+    if name == "c2":
+        # the whole image with the reference's semantics (no horizon guard): FP32
+        # against FP64 on the pixels where the FP64 method is well conditioned
+        f64 = bn.render(db, v, precision="fp64").image().cpu().numpy()
+        cond = conditioned_pixels(db, v, f64)
+        i32 = r32.image().cpu().numpy().astype(np.float64)
+        print(f"conditioned {cond.mean():.5f} rel_l1_I {rel_l1(i32[..., 0][cond], f64[..., 0][cond]):.3e} "
+              f"dm {flux_weighted_dm(i32[cond], f64[cond]):.3e}")
+        assert cond.mean() >= 0.98   # 0.9806 measured: captured rays that overshoot and spin-axis rays are the rest
+        assert rel_l1(i32[..., 0][cond], f64[..., 0][cond]) <= FP32_I_REL_L1
+        assert flux_weighted_dm(i32[cond], f64[cond]) <= FP32_DM
 
 
 def conditioned_pixels(db, view, f64_img):

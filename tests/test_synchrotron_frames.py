@@ -77,9 +77,14 @@ def test_gpu_frames_match_reference(golden, name, nu):
     model = _model(name)
     got = model.coefficients_batch(golden["frames"], nu)
     assert got.shape == ref.shape and got.dtype == np.float64
-    assert np.array_equal(got == 0.0, ref == 0.0)
+    # exact zeros agree, except where the reference's value is only the sum of
+    # its kernel table's floored tail (F, G = 1e-300 beyond x = 1e3: denormals
+    # of 1e-321 .. 1e-312 for cold, weakly magnetised frames), which the kernel
+    # leaves out and returns as 0
+    differ = (got == 0.0) != (ref == 0.0)
+    assert np.all(np.abs(ref[differ]) < 1e-290) and np.all(np.abs(got[differ]) < 1e-290)
     assert _err(got, ref) <= 1e-12
-    nz = ref != 0.0
+    nz = np.abs(ref) >= 1e-290
     assert np.max(np.abs(got[nz] - ref[nz]) / np.abs(ref[nz])) <= 1e-11
 
 
