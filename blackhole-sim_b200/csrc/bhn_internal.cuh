@@ -198,8 +198,8 @@ static_assert(sizeof(QueueState) == 64, "queue state size");
 struct ScratchLayout {
     int64_t queue, stats, raw_views, views, ray_begin, axis_begin, total;
 };
-__host__ __device__ inline ScratchLayout scratch_layout(int32_t n_views) {
-    ScratchLayout L;
+__host__ __device__ constexpr ScratchLayout scratch_layout(int32_t n_views) {
+    ScratchLayout L{};
     L.queue = 0;
     L.stats = 64;
     L.raw_views = 256;

@@ -3,12 +3,12 @@
 //
 // bhn_render_launch needs a scratch buffer (work-queue head, per-view camera
 // tables, launch totals) that the caller normally allocates.  Some callers
-// cannot: code running while a CUDA stream is being captured into a graph
-// (cudaMalloc is not allowed during capture), hosts whose device memory is
-// owned by another allocator or memory pool that must stay the only one, and
-// real-time loops that may not synchronise the device with an allocation.
-// This entry point keeps that scratch in a fixed, file-scope device array, so
-// the caller passes only its inputs and outputs.
+// cannot: hosts whose device memory is owned by their own allocator or by a
+// pool sized at start-up, where a library they load may not allocate beside
+// it, and real-time loops that may not take the device-wide synchronisation
+// that cudaMalloc / cudaFree can imply.  This entry point keeps that scratch in
+// a fixed, file-scope device array, so the caller passes only its inputs and
+// outputs.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -23,8 +23,12 @@ namespace {
 constexpr int64_t kNoAllocScratchBytes = 64 * 1024;
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+static_assert(bhn::scratch_layout(BHN_NOALLOC_MAX_VIEWS).total <= kNoAllocScratchBytes,
+              "BHN_NOALLOC_MAX_VIEWS views must fit the fixed scratch array");
+
 // Device address of g_noalloc_scratch per device (the host-side name of a
-// __device__ array is only a stand-in, never a device address).
+// __device__ array is only a stand-in, never a device address).  It is looked
+// up once per device and process; a cudaDeviceReset would invalidate it.
 constexpr int kMaxDevices = 64;
 std::atomic<void *> g_noalloc_ptr[kMaxDevices];
 
