@@ -662,6 +662,8 @@ __device__ __forceinline__ Geo camera_geo(const ViewDev &v, const CameraRay &c) 
 }
 
 // Step-doubling controller: renders the adaptive image and records samples.
+// DRIFT: track each ray's Hamiltonian drift (only when it is asked for).
+template <bool DRIFT>
 __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
     extern __shared__ __align__(16) unsigned char smem[];
     const RenderParams &P = L.R;
@@ -687,7 +689,7 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
             const CameraRay cam = camera_ray(v, px.px, px.py);
             const float pt = (float)cam.pt, pphi = (float)cam.pphi;
             Geo g = camera_geo(v, cam);
-            const float H0 = (float)cam.H0;
+            const float H0 = DRIFT ? (float)cam.H0 : 0.0f;
             float drift = 0.0f;  // max | |H| - |H0| | over the accepted steps' starts (kerr.py:352, 367)
             StokesAcc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
             // first trial step 0.05 r: the controller then tracks the accepted step
@@ -701,7 +703,7 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
                 }
                 Deriv32 k1;
                 rk2_k1(g, C, pt, pphi, k1);
-                drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
+                if constexpr (DRIFT) drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
                 h = fmaxf(brick_limit(h, g, k1, C, T, P.nr, P.nt, L.A.brick_scale), L.A.h_floor);
                 if (crosses_horizon(g, C, h, k1)) {
                     st = BHN_RAY_CAPTURED;
@@ -739,7 +741,7 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
             write_stokes(P.out, (uint32_t)px.out_idx, acc);
             if (P.ray_steps) P.ray_steps[px.out_idx] = steps;
             if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)st;
-            if (P.ray_drift) P.ray_drift[px.out_idx] = drift;
+            if constexpr (DRIFT) P.ray_drift[px.out_idx] = drift;
         }
         __syncwarp();
     }
@@ -751,7 +753,11 @@ __global__ void __launch_bounds__(256) adaptive_kernel(const LearnParams L) {
 }
 
 // The ray loop with the network's step proposal (FP32, horizon guard on).
-__global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
+// DRIFT: track each ray's Hamiltonian drift (only when it is asked for: the two
+// registers it holds cost occupancy); SUBSTEPS: RK2 steps per brick segment.
+// Five 128-thread blocks per SM: at most 102 registers a thread.
+template <bool DRIFT, int SUBSTEPS>
+__global__ void __launch_bounds__(128, 5) learned_kernel(const LearnParams L) {
     extern __shared__ __align__(16) unsigned char smem[];
     const RenderParams &P = L.R;
     Tables T;
@@ -793,7 +799,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
             const CameraRay cam = camera_ray(v, px.px, px.py);
             pt = (float)cam.pt;
             pphi = (float)cam.pphi;
-            H0 = (float)cam.H0;
+            if constexpr (DRIFT) H0 = (float)cam.H0;
             g = camera_geo(v, cam);
             if (!(v.valid && v.max_steps > 0)) alive = false, st = v.valid ? BHN_RAY_MAX_STEPS : BHN_RAY_INVALID;
         }
@@ -820,7 +826,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
             float h = fminf(fmaxf(fmaxf(mult, L.A.min_scale) * h_plain, L.A.h_floor), L.A.h_ceil);
             Deriv32 k1, k2;
             rk2_k1(g, C, pt, pphi, k1);
-            drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
+            if constexpr (DRIFT) drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
             h = fmaxf(brick_limit(h, g, k1, C, T, P.nr, P.nt, L.A.brick_scale), L.A.h_floor);
             if (crosses_horizon(g, C, h, k1)) {
                 st = BHN_RAY_CAPTURED;
@@ -840,7 +846,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
             };
             Geo y;
             float e;
-            if (L.A.substeps == 2) {
+            if constexpr (SUBSTEPS == 2) {
                 // two RK2 steps of h / 2 and one brick segment over both: the form of
                 // the controller's accepted solution, without its full-h comparison step
                 const float hh = 0.5f * h;
@@ -886,7 +892,7 @@ __global__ void __launch_bounds__(128) learned_kernel(const LearnParams L) {
             write_stokes(P.out, (uint32_t)px.out_idx, acc);
             if (P.ray_steps) P.ray_steps[px.out_idx] = steps;
             if (P.ray_status) P.ray_status[px.out_idx] = (uint8_t)st;
-            if (P.ray_drift) P.ray_drift[px.out_idx] = drift;
+            if constexpr (DRIFT) P.ray_drift[px.out_idx] = drift;
         }
         __syncwarp();
     }
@@ -1028,11 +1034,14 @@ int bhn_adaptive_launch(const void *records, const void *tables, int32_t nr, int
     L.sample_capacity = sample_capacity;
     L.counters = counters;
     const int sms = sm_count_current_device();
-    if (smem > 48 * 1024)
-        BHN_CUDA_TRY(cudaFuncSetAttribute(adaptive_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    adaptive_kernel<<<sms * cfg->blocks_per_sm, cfg->block_threads, smem, s>>>(L);
-    BHN_LAUNCH_CHECK("adaptive_kernel");
-    return BHN_OK;
+    auto go = [&](auto kernel) -> int {
+        if (smem > 48 * 1024)
+            BHN_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kernel<<<sms * cfg->blocks_per_sm, cfg->block_threads, smem, s>>>(L);
+        BHN_LAUNCH_CHECK("adaptive_kernel");
+        return BHN_OK;
+    };
+    return L.R.ray_drift ? go(adaptive_kernel<true>) : go(adaptive_kernel<false>);
 }
 
 int bhn_learned_launch(const void *records, const void *tables, int32_t nr, int32_t nt, int32_t np, int32_t n_views,
@@ -1048,12 +1057,17 @@ int bhn_learned_launch(const void *records, const void *tables, int32_t nr, int3
     L.blob = static_cast<const MlpBlob *>(blob);
     L.counters = counters;
     const int sms = sm_count_current_device();
-    if (smem > 48 * 1024)
-        BHN_CUDA_TRY(cudaFuncSetAttribute(learned_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    learned_kernel<<<sms * cfg->blocks_per_sm * (cfg->block_threads / 128 > 0 ? cfg->block_threads / 128 : 1), 128,
-                     smem, s>>>(L);
-    BHN_LAUNCH_CHECK("learned_kernel");
-    return BHN_OK;
+    const unsigned blocks = sms * cfg->blocks_per_sm * (cfg->block_threads / 128 > 0 ? cfg->block_threads / 128 : 1);
+    auto go = [&](auto kernel) -> int {
+        if (smem > 48 * 1024)
+            BHN_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        kernel<<<blocks, 128, smem, s>>>(L);
+        BHN_LAUNCH_CHECK("learned_kernel");
+        return BHN_OK;
+    };
+    const bool drift = L.R.ray_drift != nullptr;
+    if (L.A.substeps == 2) return drift ? go(learned_kernel<true, 2>) : go(learned_kernel<false, 2>);
+    return drift ? go(learned_kernel<true, 1>) : go(learned_kernel<false, 1>);
 }
 
 }  // extern "C"
