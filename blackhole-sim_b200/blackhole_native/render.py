@@ -116,14 +116,14 @@ class View:
 class RenderConfig:
     """Launch shape of the persistent kernel (see autotune.py).  The defaults
     are the autotuner's choice on B200 for a 1024x1024 image: 256-thread
-    blocks, 6 per SM, 4x8 pixel tiles, batch mode, the 80-register variant."""
+    blocks, 4 per SM, 4x8 pixel tiles, batch mode, the 64-register variant."""
 
     block_threads: int = 256
-    blocks_per_sm: int = 6
+    blocks_per_sm: int = 4
     tile_w: int = 4
     tile_h: int = 8
     refill_min: int = 32
-    reg_cap: int = 80
+    reg_cap: int = 64
 
     def to_struct(self, precision: int) -> _lib.RenderConfigStruct:
         c = _lib.RenderConfigStruct()
