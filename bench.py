@@ -426,6 +426,11 @@ def bench_ours(args) -> dict | None:
     tti = None
     if rank == 0 and world == 1 and not args.no_time_to_image:
         tti = time_to_image(device, 2048, 3)
+    # BASELINE config 4 in brief (the full record is `--workload views`): the
+    # 256 seeded uneven views in one CUDA-graph launch, aggregate rate
+    views_block = None
+    if rank == 0 and world == 1 and not args.no_views:
+        views_block = views_summary(device, K=3)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -447,6 +452,7 @@ def bench_ours(args) -> dict | None:
         "h_drift": {"max_all_rays": st2.max_h_drift, "max_escaped_rays": st2.max_h_drift_escaped},
         "accuracy": accuracy,
         "time_to_image": tti,
+        "views": views_block,
     }
     rnd.release_graph()
     if world > 1:
@@ -454,6 +460,42 @@ def bench_ours(args) -> dict | None:
 
         td.destroy_process_group()
     return line if rank == 0 else None
+
+
+def views_summary(device, K: int = 3) -> dict:
+    """The 256-view batched launch (scenes.uneven_views(256, seed=0) through the
+    shared 128x64x128x11 brick, autotuned shape, CUDA graph): ray-steps/s over
+    K timed launches after 3 warm-up launches, with its own clock record."""
+    import torch
+
+    import blackhole_native as bn
+    from blackhole_native import autotune, scenes
+
+    db = bn.DeviceBrick(scenes.shared_brick(), device=device, precisions=("fp32",))
+    views = scenes.uneven_views(256, seed=0)
+    cfg = autotune.cached_config("views256", device) or bn.RenderConfig()
+    rnd = bn.Renderer(db, views, config=cfg, precision="fp32")
+    stream = torch.cuda.current_stream(device)
+    rnd.capture()
+    for _ in range(3):
+        rnd.graph_launch()
+    torch.cuda.synchronize(device)
+    st = rnd.result().stats()
+    clocks = ClockSampler(_uuid(device)).start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        rnd.graph_launch()
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / K
+    rnd.release_graph()
+    return {"workload": "256 seeded uneven views (side 64-1024, a~U(0,0.998), incl~U(5,85)deg, "
+                        "max_steps~U{512..8192}), shared 128x64x128x11 float32 brick, one CUDA-graph launch",
+            "value": st.ray_steps / (ms * 1e-3), "unit": UNIT, "ms_per_launch": ms, "launches": K,
+            "ray_steps_per_launch": st.ray_steps, "rays": st.rays, "status_counts": st.status, "clocks": clk}
 
 
 def bench_views(args) -> dict | None:
@@ -1404,6 +1446,7 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-views", action="store_true", help="skip the 256-view block of the default line")
     ap.add_argument("--no-time-to-image", action="store_true",
                     help="skip the learned-vs-controller-vs-plain time to a 2048^2 image at 1e-3")
     ap.add_argument("--no-accuracy", action="store_true",
