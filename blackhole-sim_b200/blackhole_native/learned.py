@@ -46,7 +46,7 @@ FEATURE_NAMES = ("log_r", "cos_theta", "asinh_p_r", "asinh_p_theta", "spin_a", "
 # The spin feature is standardised with a fixed scale: training scenes span a
 # narrow band of spins and the data spread would magnify any other spin.
 FIXED_NORM = {4: (0.5, 0.5)}
-FALLBACKS = {"plain": 0, "controller": 1}
+FALLBACKS = {"plain": 0, "controller": 1, "retry": 2}
 WEIGHTS_DIR = Path(__file__).resolve().parent / "weights"
 
 
@@ -90,7 +90,8 @@ class AdaptConfig:
     min_scale: float = 0.3
     interval: int = 16
     max_attempts: int = 16
-    fallback: str = "controller"   # learned: "plain" or "controller" takes a step that fails the check
+    fallback: str = "controller"   # learned: "plain" or "controller" takes a step that fails the check, or
+                                   # "retry": the lane retries it with a shorter proposal next iteration
     seed: int = 1
     substeps: int = 1              # learned: RK2 steps of h / substeps per brick segment (1 or 2)
 

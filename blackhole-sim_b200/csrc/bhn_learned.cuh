@@ -28,7 +28,10 @@
 //     checks every proposal; where it fails (the network mispredicts, e.g.
 //     rays grazing the spin axis) either the plain step (fallback 0) or the
 //     step-doubling controller, started from 0.9 e^(-1/2) h (fallback 1),
-//     takes that step.
+//     takes that step, or (fallback 2) the step is not taken and that lane
+//     tries it again next iteration with the proposal cut by 0.9 e^(-1/2), at
+//     most max_attempts times.  With substeps = 2 a proposal is taken as two
+//     RK2 steps of h / 2 under one brick segment, each half step checked.
 //   * Both tracers cap steps inside the brick (brick_limit) and keep the
 //     plain tracers' horizon guard (crosses_horizon).
 
@@ -347,8 +350,8 @@ struct AdaptParams {
     float brick_scale;  // in-brick step cap as a multiple of the plain step (0: none)
     float min_scale;    // learned: the step is at least min_scale times the plain step
     int interval;       // learned: steps between network evaluations
-    int max_attempts;   // adaptive: attempts per step before forcing acceptance
-    int fallback;       // learned: a failed check takes the plain step (0) or the controller's (1)
+    int max_attempts;   // attempts per step before forcing acceptance (controller; learned retry)
+    int fallback;       // learned: a failed check takes the plain step (0), the controller's (1), or retries (2)
     uint32_t seed;
     int substeps;       // learned: RK2 steps of h / substeps per brick segment (1 or 2)
 };
@@ -790,6 +793,8 @@ __global__ void __launch_bounds__(128, 5) learned_kernel(const LearnParams L) {
         px.out_idx = 0;
         Geo g = {1000.f, 0.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         float pt = -1.0f, pphi = 0.0f, mult = 1.0f, H0 = 0.0f, drift = 0.0f;
+        float shrink = 1.0f;  // retry fallback: this lane's cut of the proposal since the last evaluation
+        int fails = 0;        // retry fallback: failed attempts at the current step
         StokesAcc acc = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, false};
         int steps = 0, st = -1;
         if (alive) {
@@ -812,6 +817,7 @@ __global__ void __launch_bounds__(128, 5) learned_kernel(const LearnParams L) {
                 for (int q = 0; q < 8; ++q) f[q] = alive ? (f[q] - N.mu_x[q]) * N.inv_sx[q] : 0.0f;
                 const float y = mlp_warp_infer(f, sb, xs, ys);
                 mult = __expf(fmaf(N.sig_y, y, N.mu_y) - L.A.margin);
+                shrink = 1.0f;
                 ++n_net;
             }
             if (!alive) continue;
@@ -823,7 +829,7 @@ __global__ void __launch_bounds__(128, 5) learned_kernel(const LearnParams L) {
             const float r0 = g.rh + g.rl;
             // the network's multiplier applies to the plain step at the current r
             const float h_plain = fminf(fmaxf(C.hs * r0, C.hmin), C.hmax);
-            float h = fminf(fmaxf(fmaxf(mult, L.A.min_scale) * h_plain, L.A.h_floor), L.A.h_ceil);
+            float h = fminf(fmaxf(fmaxf(mult, L.A.min_scale) * shrink * h_plain, L.A.h_floor), L.A.h_ceil);
             Deriv32 k1, k2;
             rk2_k1(g, C, pt, pphi, k1);
             if constexpr (DRIFT) drift = fmaxf(drift, fabsf(fabsf(k1.H) - H0));
@@ -857,14 +863,24 @@ __global__ void __launch_bounds__(128, 5) learned_kernel(const LearnParams L) {
                 rk2_stages(ym, hh, C, pt, pphi, k1b, k2b, true);
                 e = fmaxf(e, check(ym, hh, k1b, k2b));
                 n_eval += 4;
-                if (!(e > 1.0f)) y = geo_advance(ym, hh, k2b);
+                if (!(e > 1.0f) || L.A.fallback == 2) y = geo_advance(ym, hh, k2b);
             } else {
                 rk2_stages(g, h, C, pt, pphi, k1, k2, false);
                 n_eval += 2;
                 e = check(g, h, k1, k2);
-                if (!(e > 1.0f)) y = geo_advance(g, h, k2);
+                if (!(e > 1.0f) || L.A.fallback == 2) y = geo_advance(g, h, k2);
             }
-            if (e > 1.0f) {
+            if (e > 1.0f && L.A.fallback == 2) {
+                // misprediction, retry form: the step is not taken; this lane takes it
+                // again next iteration with a shorter proposal (every lane of the warp
+                // runs the same step each iteration, so nothing waits on a fallback
+                // path).  After max_attempts tries, or at h_floor, the step is taken.
+                ++n_fb;
+                if (++fails < L.A.max_attempts && h > L.A.h_floor) {
+                    shrink *= fmaxf(0.2f, 0.9f * rsqrtf(e));
+                    continue;
+                }
+            } else if (e > 1.0f) {
                 ++n_fb;
                 if (L.A.fallback == 0) {  // misprediction: the plain step
                     ++n_eval;
@@ -883,6 +899,7 @@ __global__ void __launch_bounds__(128, 5) learned_kernel(const LearnParams L) {
             brick_segment(T, rec, P.nr, P.nt, P.np, C, g, y, dr, dph_u, acc);
             const bool finite = isfinite(y.rh + y.th_h + y.ph_h + y.pr + y.pth);
             g = y;
+            fails = 0;
             ++steps;
             ++n_acc;
             st = terminate(g, C, acc, dr, finite, steps);
@@ -916,7 +933,7 @@ static int learn_params(const void *records, const void *tables, int32_t nr, int
     if (rc) return rc;
     if (!ap) return fail(BHN_ERR_VALUE, "adapt params must not be NULL");
     if (!(ap->tol > 0.0f) || !(ap->h_floor > 0.0f) || !(ap->h_ceil >= ap->h_floor) || ap->interval < 1 ||
-        ap->max_attempts < 1 || (ap->fallback != 0 && ap->fallback != 1) || !(ap->sample_prob >= 0.0f) ||
+        ap->max_attempts < 1 || ap->fallback < 0 || ap->fallback > 2 || !(ap->sample_prob >= 0.0f) ||
         !(ap->check_tol >= 0.0f) || !(ap->min_scale > 0.0f) || (ap->substeps != 1 && ap->substeps != 2))
         return fail(BHN_ERR_VALUE, "adapt params: need tol > 0, 0 < h_floor <= h_ceil, check_tol >= 0, min_scale > 0, "
                                    "max_attempts >= 1, substeps 1 or 2");

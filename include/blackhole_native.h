@@ -287,7 +287,8 @@ typedef struct bhn_adapt_params {
     float min_scale;     /* learned: the step is at least min_scale times the plain step (> 0) */
     int32_t interval;    /* learned: steps between network evaluations (the multiplier is kept in between) */
     int32_t max_attempts; /* controller: attempts per step before the step is forced */
-    int32_t fallback;    /* learned: a step failing the check is the plain step (0) or the controller's (1) */
+    int32_t fallback;    /* learned: a step failing the check is the plain step (0), the controller's (1), or
+                            retried by the lane with a shorter proposal next iteration (2; at most max_attempts) */
     uint32_t seed;       /* controller: sample-selection hash seed */
     int32_t substeps;    /* learned: 1 = one RK2 step of the proposed h per brick segment; 2 = two RK2 steps of
                             h / 2 per segment (the controller's accepted-solution form, without its h-step
