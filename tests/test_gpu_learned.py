@@ -127,3 +127,40 @@ def test_learned_gain_over_plain():
     assert e_learn <= 1.25 * e_plain + 2e-5, (e_learn, e_plain)
     assert run.counters["rhs_evals"] <= plain.counters["rhs_evals"] / 3, (run.counters, plain.counters)
     assert run.counters["net_evals_per_warp"] > 0
+
+
+@pytest.mark.parametrize("substeps,fallback", [(2, "controller"), (1, "retry"), (2, "retry")])
+def test_learned_loop_forms(scene3, substeps, fallback):
+    """The two-half-step form and the retry fallback: finite images, per-ray
+    Hamiltonian drift reported, counters consistent (a two-half-step proposal
+    costs four RHS evaluations, a retried one is not counted as a step), and
+    the image within the 1e-3 Stokes-I bar of the FP64 kernel at h/8 on the
+    pixels both agree to converge."""
+    from blackhole_native import studies
+
+    net = learned.shipped_weights()
+    v = bn.View(64, 64, spin_a=0.998, inclination_deg=60.0, max_steps=65536, horizon_guard=True)
+    cfg = learned.AdaptConfig(substeps=substeps, fallback=fallback, max_attempts=6, check_tol=1e-3)
+    run = learned.render_learned(scene3, [v], net, cfg, ray_outputs=True)
+    img = run.image().cpu().numpy()
+    assert np.all(np.isfinite(img))
+    res = run.renderer.result()
+    drift = res.per_ray("h_drift").cpu().numpy()
+    status = res.per_ray("status").cpu().numpy()
+    assert np.all(np.isfinite(drift)) and np.median(drift[status == 2]) < 1e-3
+    c = run.counters
+    assert c["steps"] > 0 and c["rhs_evals"] >= 2 * substeps * (c["steps"] - c["fallbacks"])
+    ref = bn.render(scene3, v.scaled_step(1 / 8), precision="fp64").image().cpu().numpy()
+    ref16 = bn.render(scene3, v.scaled_step(1 / 16), precision="fp64").image().cpu().numpy()
+    scale = studies.median_lit(ref16[..., 0])
+    mask = np.abs(ref[..., 0] - ref16[..., 0]) <= 1e-2 * np.abs(ref16[..., 0]) + 1e-4 * scale
+    assert mask.mean() >= 0.9
+    e = studies.image_errors(img, ref16, mask, scale)
+    assert e["capped_rel_l1_I"] <= 1e-2, e
+
+
+def test_retry_fallback_rejects_bad_params(scene3):
+    with pytest.raises(ValueError):
+        learned.AdaptConfig(fallback="sometimes").to_struct()
+    with pytest.raises(ValueError):
+        learned.AdaptConfig(substeps=3).to_struct()
