@@ -73,27 +73,31 @@ class AdaptStruct(ctypes.Structure):
 @dataclass(frozen=True)
 class AdaptConfig:
     """Parameters of the step-doubling controller and of the learned loop
-    (``bhn_adapt_params``).  The defaults are the learned loop's measured
-    operating point: proposals at the network's h_opt (margin 0) with a floor
-    of 0.3 plain steps, network evaluated every 16 steps (every 4 gives the
-    same images 1.3x slower: one evaluation costs about one RK2 step of the
-    warp), Euler-midpoint check at 1e-3 with the controller as fallback,
-    in-brick steps no longer than the plain step."""
+    (``bhn_adapt_params``).  The learned loop's defaults are its measured
+    operating point on the 2048^2 time-to-image scenes: each proposal taken as
+    two RK2 steps of h / 2 under one brick segment (``substeps=2``), proposals
+    at exp(-0.6) of the network's h_opt, floored at 0.3 plain steps, the
+    Euler-midpoint check at 1e-3 on each half step, and a failing proposal
+    retried by its lane with a shorter step (``fallback="retry"``: the plain
+    RK2 step again, at most ``max_attempts`` times -- 16, the controller's
+    attempt limit too), so every lane of a warp runs the same step; the
+    network is evaluated every 16 steps (one evaluation costs about one RK2
+    step of the warp); in-brick steps are no longer than the plain step."""
 
     tol: float = 1e-4
     sample_prob: float = 0.0
     h_floor: float = 1e-6
     h_ceil: float = 64.0
-    margin: float = 0.0
+    margin: float = 0.6
     check_tol: float = 1e-3
     brick_scale: float = 1.0
     min_scale: float = 0.3
     interval: int = 16
     max_attempts: int = 16
-    fallback: str = "controller"   # learned: "plain" or "controller" takes a step that fails the check, or
-                                   # "retry": the lane retries it with a shorter proposal next iteration
+    fallback: str = "retry"        # learned: "retry" -- the lane retries a failing proposal with a shorter
+                                   # step next iteration -- or "plain" / "controller" takes that step
     seed: int = 1
-    substeps: int = 1              # learned: RK2 steps of h / substeps per brick segment (1 or 2)
+    substeps: int = 2              # learned: RK2 steps of h / substeps per brick segment (1 or 2)
 
     def to_struct(self) -> AdaptStruct:
         if self.fallback not in FALLBACKS:

@@ -256,7 +256,7 @@ def learned_study(net: learned.StepNet, side: int = 2048, log=print,
             for tol in (1e-4, 1e-5):
                 record("controller", {"tol": tol, "brick_scale": bs},
                        learned.render_adaptive(db, [v], learned.AdaptConfig(tol=tol, brick_scale=bs), repeats=3))
-            for fb in ("controller", "plain"):
+            for fb in ("retry", "controller", "plain"):
                 record("learned", {"fallback": fb, "brick_scale": bs},
                        learned.render_learned(db, [v], net, learned.AdaptConfig(brick_scale=bs, fallback=fb), repeats=3))
         best = {}

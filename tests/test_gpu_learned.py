@@ -119,7 +119,8 @@ def test_learned_gain_over_plain():
         np.abs(ref8[..., 0] - ref[..., 0]) <= 1e-2 * np.abs(ref[..., 0]) + 1e-4 * scale)
     assert mask.mean() >= 0.98
     plain = learned.render_plain(db, [v.scaled_step(0.25)])
-    run = learned.render_learned(db, [v], net, learned.AdaptConfig(brick_scale=0.25))
+    run = learned.render_learned(db, [v], net, learned.AdaptConfig(brick_scale=0.25, substeps=1, margin=0.0,
+                                                                  fallback="controller"))
     img = run.image().cpu().numpy()
     assert np.all(np.isfinite(img))
     e_plain = studies.image_errors(plain.image().cpu().numpy(), ref, mask, scale)["capped_rel_l1_I"]
