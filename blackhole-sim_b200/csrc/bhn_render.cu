@@ -317,6 +317,8 @@ constexpr double kNearHorizon = 0.1;  // FP64 island: steps that start within 0.
 // whose FP32 result overflows.
 constexpr float kPoleIsland = 1.0e-4f;
 constexpr float kMomentumIsland = 1.0e15f;
+// Tracer32::step's answer for a step that belongs to an FP64 island.
+constexpr int kNeedFp64 = -2;
 
 // ------------------------------------------------------------ FP64 helpers
 struct Deriv64 {
@@ -506,6 +508,7 @@ __device__ __forceinline__ void rhs64h(double r, double th_in, double pr, double
 }
 
 struct Tracer32 {
+    static constexpr bool kIslands = true;  // step may answer kNeedFp64
     float rh, rl, th_h, th_l, ph_h, ph_l;  // positions as compensated pairs (value = hi + lo)
     float pr, pth, pt, pphi;
     float S0, S1, S2, S3, tau, drift, H0;
@@ -538,7 +541,9 @@ struct Tracer32 {
     // Returns 0 (finite), 1 (non-finite) or 2 (horizon guard: the midpoint lies
     // inside the horizon; the state is left unchanged).
     // Not inlined: the FP64 step runs for a few steps in a thousand, and keeping
-    // its code out of the FP32 loop keeps that loop's registers for itself.
+    // its code out of the FP32 loop keeps that loop's registers for itself.  It
+    // is only ever called on a copy of the tracer (step64), so the tracer that
+    // the FP32 loop carries is never address-taken and stays in registers.
     __device__ __noinline__ int step_fp64(const ViewDev &v, bool guard, float &dr, float &dph) {
         const double r = (double)rh + (double)rl;
         const double th = (double)th_h + (double)th_l;
@@ -568,13 +573,14 @@ struct Tracer32 {
     }
 
     // One RK2 geodesic step plus its brick segment.  Returns -1 while the ray
-    // lives, else its BHN_RAY_* status.
+    // lives, kNeedFp64 (state untouched) when the step belongs to an FP64
+    // island -- the caller then takes it with step64, outside its FP32 loop --
+    // else the ray's BHN_RAY_* status.
     __device__ __forceinline__ int step(const StepConst &C, const Tables &T, const float4 *__restrict__ rec, int nr,
                                         int nt, int np, const ViewDev *__restrict__ views) {
         if (rh < C.r_guard && pr < 0.0f) return BHN_RAY_CAPTURED;  // horizon guard (flag; off by default)
         const float r0 = rh + rl, th0 = th_h + th_l, ph0 = ph_h + ph_l;
         float dr = 0.0f, dph = 0.0f;
-        bool finite = true;
         const bool south = th_h > kHalfPiF;
         const float d0 = south ? (kPiH - th_h) + (kPiL - th_l) : th0;
         bool fp64 = rh < C.r_near || d0 < kPoleIsland || !(fabsf(pth) < kMomentumIsland && fabsf(pr) < kMomentumIsland);
@@ -619,11 +625,28 @@ struct Tracer32 {
                 }
             }
         }
-        if (fp64) {
-            const int rc = step_fp64(views[vi], C.r_guard > 0.0f, dr, dph);
-            if (rc == 2) return BHN_RAY_CAPTURED;
-            finite = rc == 0;
-        }
+        if (fp64) return kNeedFp64;
+        return segment(C, T, rec, nr, nt, np, r0, th0, ph0, dr, dph, true);
+    }
+
+    // The step in FP64 (an island), then its brick segment; returns like step.
+    __device__ __forceinline__ int step64(const StepConst &C, const Tables &T, const float4 *__restrict__ rec, int nr,
+                                          int nt, int np, const ViewDev *__restrict__ views) {
+        const float r0 = rh + rl, th0 = th_h + th_l, ph0 = ph_h + ph_l;
+        float dr = 0.0f, dph = 0.0f;
+        Tracer32 t = *this;
+        const int rc = t.step_fp64(views[vi], C.r_guard > 0.0f, dr, dph);
+        *this = t;
+        if (rc == 2) return BHN_RAY_CAPTURED;
+        return segment(C, T, rec, nr, nt, np, r0, th0, ph0, dr, dph, rc == 0);
+    }
+
+    // Everything after the geodesic update: the step count, phi back into
+    // [0, 2 pi), the segment from (r0, th0, ph0) to the new state, and the
+    // stopping rules.
+    __device__ __forceinline__ int segment(const StepConst &C, const Tables &T, const float4 *__restrict__ rec, int nr,
+                                           int nt, int np, float r0, float th0, float ph0, float dr, float dph,
+                                           bool finite) {
         ++steps;
         const float th1 = th_h + th_l;
         // phi is only sampled modulo 2 pi: keep the state in [0, 2 pi)
@@ -757,6 +780,7 @@ struct Tracer32 {
 
 // ------------------------------------------------------------ FP64 tracer
 struct Tracer64 {
+    static constexpr bool kIslands = false;  // step never answers kNeedFp64
     double r, th, ph, pr, pth, pt, pphi;
     double S0, S1, S2, S3, tau, drift, H0;
     int steps, brick, vi;
@@ -985,9 +1009,20 @@ __global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P)
                 tr.init(v, vi, px.px, px.py, px.out_idx);
                 const StepConst &C = sconst[vi];
                 int st;
-                do {
-                    st = tr.step(C, T, rec, P.nr, P.nt, P.np, P.views);
-                } while (st < 0);
+                // the FP32 steps in a tight inner loop; an island step leaves it
+                // for the out-of-line FP64 step and comes back
+                for (;;) {
+                    do {
+                        st = tr.step(C, T, rec, P.nr, P.nt, P.np, P.views);
+                    } while (st == -1);
+                    if constexpr (Tracer::kIslands) {
+                        if (st != kNeedFp64) break;
+                        st = tr.step64(C, T, rec, P.nr, P.nt, P.np, P.views);
+                        if (st != -1) break;
+                    } else {
+                        break;
+                    }
+                }
                 tr.finish(P.out, st, C, P.views);
                 const float d = tr.drift_f();
                 atomicAdd(&bc->steps, (unsigned long long)tr.steps);
@@ -1055,7 +1090,10 @@ __global__ void __launch_bounds__(256, MINB) render_kernel(const RenderParams P)
         }
         if (alive) {
             const StepConst &C = sconst[tr.vi];
-            const int st = tr.step(C, T, rec, P.nr, P.nt, P.np, P.views);
+            int st = tr.step(C, T, rec, P.nr, P.nt, P.np, P.views);
+            if constexpr (Tracer::kIslands) {
+                if (st == kNeedFp64) st = tr.step64(C, T, rec, P.nr, P.nt, P.np, P.views);
+            }
             if (st >= 0) {
                 tr.finish(P.out, st, C, P.views);
                 const float d = tr.drift_f();
