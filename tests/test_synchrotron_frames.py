@@ -70,6 +70,30 @@ def _model(name):
     return T if T is not None else N
 
 
+def test_kernel_table_first_guess_is_within_one_segment():
+    """The device lookup of the F / G table takes the segment guess
+    (lx - lx[0]) * inv and corrects it by at most one knot each way.  That is
+    exact when the guess is never off by more than one, which holds for the
+    table's log-uniform knots (log of the geomspace(1e-8, 1e3, 256) built like
+    the device table): checked at the knots, their float neighbours and a
+    million random points against numpy's searchsorted (numpy.interp's
+    segment)."""
+    n = 256
+    ls, le = np.log10(1.0e-8), np.log10(1.0e3)
+    step = (le - ls) / (n - 1)
+    x = 10.0 ** (np.arange(n) * step + ls)
+    x[0], x[-1] = 1.0e-8, 1.0e3
+    lx = np.log(x)
+    inv = (n - 1) / (lx[-1] - lx[0])
+    rng = np.random.default_rng(7)
+    pts = np.concatenate([lx, np.nextafter(lx, -np.inf), np.nextafter(lx, np.inf),
+                          rng.uniform(lx[0], lx[-1], 1_000_000)])
+    pts = np.clip(pts, lx[0], lx[-1])
+    guess = np.clip(((pts - lx[0]) * inv).astype(np.int64), 0, n - 2)
+    true = np.clip(np.searchsorted(lx, pts, side="right") - 1, 0, n - 2)
+    assert np.abs(guess - true).max() <= 1
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,nu", CASES)
 def test_gpu_frames_match_reference(golden, name, nu):
