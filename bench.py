@@ -991,8 +991,10 @@ def bench_bricks(args) -> dict | None:
     db = acc.DeviceBricks(grid, device)
     pixels = cfg.width * cfg.height
     img, diag = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True)
+    full_img, full_diag = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True, full_trace=True)
     torch.cuda.synchronize(device)
-    d = diag.cpu().numpy()
+    assert torch.equal(full_img, img), "the outbound exit changed the image"
+    d, fd = diag.cpu().numpy(), full_diag.cpu().numpy()
     steps, segments = float(d[..., 2].sum()), float(d[..., 1].sum())
     peaks = fp64_peaks(device, stream)
     for _ in range(args.warmup):
@@ -1008,6 +1010,12 @@ def bench_bricks(args) -> dict | None:
     assert all(torch.equal(o, img) for o in outs), "images differ between launches"
     t_max = max_over_ranks(sum(per), world, device)
     value = sum_over_ranks(pixels * args.steps, world, device) / (t_max * 1e-3)
+    # the same image with every ray traced to the reference's own end (escape radius 220, capture, max_steps)
+    per_full = timed_launches(lambda: acc.render_stokes_image_bricks_device(cfg, snap, db, full_trace=True),
+                              args.steps, stream, device)
+    full_trace = {"ms_per_step": statistics.mean(per_full), "pixels_per_s": pixels / (statistics.mean(per_full) * 1e-3),
+                  "rk4_steps_per_step": float(fd[..., 2].sum()), "longest_ray_steps": int(fd[..., 2].max()),
+                  "note": "full_trace=True: rays also traced past the brick to the escape radius; same image"}
 
     e2e = None
     if not args.no_e2e:  # public API: host brick in (float32, uploaded and widened on the device), host image out
@@ -1042,6 +1050,9 @@ def bench_bricks(args) -> dict | None:
                                "pixels, camera r=55M i=65deg FOV 32deg, RK4 step 0.06, 5000 steps, RK2 Stokes "
                                f"steps, seeded {B['nr']}x{B['ntheta']}x{B['nphi']}x11 float32 torus brick",
                    "pixels_per_step": pixels, "rk4_steps_per_step": steps, "sampled_segments_per_step": segments,
+                   "longest_ray_steps": int(d[..., 2].max()),
+                   "outbound_exit": "a ray past the brick's outer radius moving out with no radial turning point "
+                                    "ahead ends there (nothing later is sampled; image bit-identical to full traces)",
                    "l2": "brick (92 MB of float64 coefficients) resident in L2 between launches; the rays read "
                          "at most a few cells per step",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -1056,6 +1067,7 @@ def bench_bricks(args) -> dict | None:
                      "flop_per_rk4_step": FP64_FLOP_PER_RK4_STEP, "flop_per_segment": FP64_FLOP_PER_SEGMENT},
         "cpu_baseline": cpu,
         "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
+        "full_trace": full_trace,
     }
     if world > 1:
         import torch.distributed as td

@@ -55,6 +55,7 @@ class BrickTraceConfigStruct(ctypes.Structure):
         ("max_optical_depth", ctypes.c_double),
         ("max_steps", ctypes.c_int32),
         ("exact_step", ctypes.c_int32),
+        ("full_trace", ctypes.c_int32),
     ]
 
 
@@ -99,7 +100,7 @@ class DeviceBricks:
         self.coeffs = torch.from_numpy(src).to(self.device).to(torch.float64)
 
 
-def _view_and_config(cfg, snapshot, tile):
+def _view_and_config(cfg, snapshot, tile, full_trace=False):
     """The bhn_view (camera, crop) and bhn_brick_trace_config of one call, checked on the host."""
     W, H = int(cfg.width), int(cfg.height)
     if W < 1 or H < 1:
@@ -126,17 +127,25 @@ def _view_and_config(cfg, snapshot, tile):
     c.length_cm = float(getattr(t, "affine_to_length_cm", None) or 1.0)  # accelerated_renderer.py:146
     c.max_optical_depth, c.max_steps = float(t.max_optical_depth), int(cfg.max_steps)
     c.exact_step = int(bool(t.use_exact_matrix_step))
+    c.full_trace = int(bool(full_trace))
     return v, c, (h, w)
 
 
 def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagnostics: bool = False,
-                                      device: torch.device | None = None):
+                                      device: torch.device | None = None, full_trace: bool = False):
     """(h, w, 4) float64 Stokes image of the tile (default: the whole image)
     on the device, and (h, w, 4) diagnostics (columns ``DIAGNOSTICS``) when
     asked.  ``snapshot`` supplies the spin (``spin_a``); ``bricks`` is a
-    ``CoefficientBrickGrid``-like object or a ``DeviceBricks``."""
+    ``CoefficientBrickGrid``-like object or a ``DeviceBricks``.
+
+    A ray's trace ends where the reference's does (capture, escape radius,
+    max_steps, non-finite state), at the optical-depth cutoff, or -- unless
+    ``full_trace`` -- once it is past the brick's outer radius moving out with
+    no radial turning point ahead (status ``outbound``): nothing after either
+    cutoff is sampled, so the image is the same; only the diagnostics' step
+    count and status differ from a full trace's."""
     # host-side checks first: a bad call fails the same way with or without a GPU
-    v, c, (h, w) = _view_and_config(cfg, snapshot, tile)
+    v, c, (h, w) = _view_and_config(cfg, snapshot, tile, full_trace)
     if not isinstance(bricks, DeviceBricks):
         bricks = DeviceBricks(bricks, device)
     device = bricks.device

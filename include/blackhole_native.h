@@ -37,13 +37,16 @@ typedef enum bhn_status {
 enum { BHN_POLICY_NAN = 0, BHN_POLICY_INITIAL = 1, BHN_POLICY_ZERO = 2 };
 
 /* Ray termination status (kerr.py:25 plus the optical-depth cutoff of
- * accelerated_renderer.py:123-125). */
+ * accelerated_renderer.py:123-125).  BHN_RAY_OUTBOUND (brick renderer only):
+ * the ray is past the brick's outer radius, moving out, and can never turn
+ * back, so no later segment is sampled and its image is final. */
 enum {
     BHN_RAY_MAX_STEPS = 0,
     BHN_RAY_CAPTURED = 1,
     BHN_RAY_ESCAPED = 2,
     BHN_RAY_INVALID = 3,
-    BHN_RAY_OPAQUE = 4
+    BHN_RAY_OPAQUE = 4,
+    BHN_RAY_OUTBOUND = 5
 };
 
 /* ---- library ------------------------------------------------------------ */
@@ -412,6 +415,12 @@ int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, cons
  * is the RK2, h = 0.02 r form of the same loop.)  coeffs: [nr][nt][np][11]
  * float64; out: [rays][4] at view->out_offset; diag (optional): [rays][4] =
  * optical depth, sampled segments, RK4 steps taken, BHN_RAY_* status.
+ * Unless full_trace is set, a ray's trace also ends once it is past the
+ * brick's outer radius, moving out, with a radial potential that keeps it
+ * moving out (R(r') >= E^2 r'^4 / 4 for every r' beyond it: status
+ * BHN_RAY_OUTBOUND): no later segment can be sampled, so the image is the
+ * same bit for bit, and only the diag columns "RK4 steps taken" and
+ * "status" differ from the full trace's.
  * scratch: bhn_render_scratch_bytes(1). */
 typedef struct bhn_brick_trace_config {
     double step;                 /* affine RK4 step (AcceleratedRenderConfig.step) */
@@ -420,6 +429,8 @@ typedef struct bhn_brick_trace_config {
     double max_optical_depth;
     int32_t max_steps;
     int32_t exact_step;          /* 1: stokes_step_exact, 0: RK2 */
+    int32_t full_trace;          /* 1: trace every ray to the reference's own end (escape radius, capture,
+                                    max_steps), 0: also end outbound rays past the brick (same image) */
 } bhn_brick_trace_config;
 int bhn_brick_trace_render(const double *coeffs, const double *r_grid, int32_t nr, const double *theta_grid,
                            int32_t nt, const double *phi_grid, int32_t np, const bhn_view *view,

@@ -190,14 +190,15 @@ def test_config_struct_layout_matches_ctypes(tmp_path):
     include = Path(__file__).resolve().parents[1] / "include"
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "blackhole_native.h"\n'
-                   'int main(void){printf("%zu %zu %zu\\n", sizeof(bhn_brick_trace_config),'
-                   ' offsetof(bhn_brick_trace_config, max_steps), offsetof(bhn_brick_trace_config, exact_step));'
+                   'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(bhn_brick_trace_config),'
+                   ' offsetof(bhn_brick_trace_config, max_steps), offsetof(bhn_brick_trace_config, exact_step),'
+                   ' offsetof(bhn_brick_trace_config, full_trace));'
                    ' return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", str(include), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     S = acc.BrickTraceConfigStruct
-    assert got == [ctypes.sizeof(S), S.max_steps.offset, S.exact_step.offset]
+    assert got == [ctypes.sizeof(S), S.max_steps.offset, S.exact_step.offset, S.full_trace.offset]
 
 
 @pytest.mark.gpu
@@ -292,3 +293,103 @@ def test_gpu_reference_regression_chain(regression, tmp_path):
     c = acc.sample_coefficient_brick(grid, *g["sample_point"])
     assert c is not None and c.shape == (11,) and _rel(c, g["sample_value"]) <= TOL
     assert acc.sample_coefficient_brick(grid, 1.0e3, 1.0, 1.0) is None
+
+
+def _default_scene_view(stride_w=160, stride_h=90):
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = 0.9375, 55.0, np.radians(65.0), 0.0
+    v.fov_y_deg, v.roll_deg, v.width, v.height = 32.0, 0.0, stride_w, stride_h
+    return v
+
+
+def _outbound_cases(golden):
+    """(view, step, max_steps, r_edge, pixels): the golden scene, and every
+    fourth row and column of the reference's default 160 x 90 image through
+    the 40 M torus brick."""
+    from blackhole_native import bricks
+
+    cam = golden["acc_cam"]
+    v = O.View()
+    v.spin_a, v.r_obs, v.theta_obs, v.phi_obs = 0.9375, cam[0], cam[1], cam[2]
+    v.fov_y_deg, v.roll_deg, v.width, v.height = cam[3], 0.0, 24, 16
+    yield v, 0.1, 900, float(_grids(golden)[0].max()), [(x, y) for y in range(16) for x in range(24)]
+    r_edge = float(np.asarray(bricks.torus_grids(128, 64, 128, 0.9375)[0], dtype=np.float32).max())
+    yield _default_scene_view(), 0.06, 5000, r_edge, [(x, y) for y in range(0, 90, 4) for x in range(0, 160, 4)]
+
+
+def test_outbound_exit_rule_on_full_oracle_traces(golden):
+    """The brick renderer ends a ray once it is past the brick's outer radius
+    moving out with R(r') >= E^2 r'^4 / 4 ahead (oracle.bricktrace.outbound_for_good
+    restates the kernel's test).  On full oracle traces of both scenes no
+    state after the first one the rule accepts lies at or inside the brick's
+    outer radius or has r falling, so no later segment could have been
+    sampled; the rule fires on most rays and shortens the longest trace."""
+    for v, h, max_steps, r_edge, pixels in _outbound_cases(golden):
+        full, cut, fired = [], [], 0
+        for px, py in pixels:
+            y0, pt, pphi = O.camera_ray(v, 2.0 * (px + 0.5) / v.width - 1.0, 1.0 - 2.0 * (py + 0.5) / v.height,
+                                        v.width / v.height)
+            st, _ = O.trace_rk4(y0, pt, pphi, v.spin_a, h, max_steps, 220.0)
+            fire = B.outbound_for_good(st[1:], pt, pphi, v.spin_a, r_edge)
+            k = int(np.argmax(fire)) + 1 if fire.any() else len(st) - 1
+            fired += bool(fire.any())
+            rest = st[k:, 1]
+            assert not np.any(rest[1:] <= r_edge) and not np.any(np.diff(rest) <= 0.0), (px, py, k)
+            full.append(len(st) - 1)
+            cut.append(k)
+        assert fired >= len(pixels) // 2
+        assert max(cut) < max(full)
+    # the default scene's longest trace: 4,798 steps in full, 1,734 to the exit (every fourth pixel)
+    assert max(cut) < 0.5 * max(full)
+
+
+def test_outbound_rule_declines_inbound_inside_and_near_periapsis():
+    """Equatorial photons (p_theta = 0, E = 1) at r = 50 past a 40 M brick:
+    the rule accepts an outward ray of small impact parameter and declines an
+    inward one, one inside the brick, and an outward ray just past its
+    periapsis (L = 48 ~ r), where R(r') >= E^2 r'^4 / 4 does not hold yet --
+    such a ray escapes too, but the rule waits until the margin does."""
+    a, E = 0.9375, 1.0
+    r, th = 50.0, np.pi / 2
+    # L chosen so that R(r) is small but positive at r (near a turning point) and dr/dlambda > 0
+    for L, pr_sign, r0, want in ((3.0, 1.0, r, True), (3.0, -1.0, r, False), (3.0, 1.0, 30.0, False),
+                                 (48.0, 1.0, r, False)):
+        u, a2 = r0 * r0, a * a
+        dlt = u - 2.0 * r0 + a2
+        K = (L - a * E) ** 2  # p_theta = 0 on the equator
+        R = (E * (u + a2) - a * L) ** 2 - dlt * K
+        pr = pr_sign * np.sqrt(max(R, 0.0)) / dlt
+        st = np.array([[0.0, r0, th, 0.0, pr, 0.0]])
+        assert bool(B.outbound_for_good(st, -E, L, a, 40.0)[0]) is want, (L, pr_sign, r0)
+
+
+@pytest.mark.gpu
+def test_gpu_outbound_exit_keeps_the_image(golden):
+    """The early exit changes no pixel: bit-identical images, optical depths
+    and sampled-segment counts against full traces (full_trace=True), on the
+    golden scene (with and without the optical-depth cutoff) and on the
+    reference's default 160 x 90 image of the seeded 128 x 64 x 128 torus
+    brick; rays ended outbound are ones the full trace ends as escaped or at
+    max_steps, after no more steps."""
+    import torch
+
+    from blackhole_native import accelerated as acc
+    from blackhole_native import bricks
+
+    snap = SimpleNamespace(spin_a=0.9375)
+    b = bricks.torus_brick(128, 64, 128, spin_a=0.9375, seed=0, dtype=np.float32)
+    scenes = [(_config(acc, golden["acc_cam"], "rk2", cut), _golden_bricks(golden)) for cut in ("full", "cut")]
+    scenes.append((acc.AcceleratedRenderConfig(), SimpleNamespace(r=b.r, theta=b.theta, phi=b.phi, coeffs=b.coeffs)))
+    outbound = 0
+    for cfg, grid in scenes:
+        db = acc.DeviceBricks(grid)
+        img, diag = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True)
+        ref, rdiag = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True, full_trace=True)
+        assert torch.equal(img, ref)
+        assert torch.equal(diag[..., :2], rdiag[..., :2])
+        st, rst = diag[..., 3].cpu().numpy(), rdiag[..., 3].cpu().numpy()
+        out = st == 5  # BHN_RAY_OUTBOUND
+        assert np.all(st[~out] == rst[~out]) and np.all(np.isin(rst[out], (0, 2)))
+        assert torch.all(diag[..., 2] <= rdiag[..., 2]) and not np.any(rst == 5)
+        outbound += int(out.sum())
+    assert outbound > 0.5 * 160 * 90
