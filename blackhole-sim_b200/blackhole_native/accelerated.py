@@ -56,6 +56,7 @@ class BrickTraceConfigStruct(ctypes.Structure):
         ("max_steps", ctypes.c_int32),
         ("exact_step", ctypes.c_int32),
         ("full_trace", ctypes.c_int32),
+        ("coeff_layout", ctypes.c_int32),
     ]
 
 
@@ -80,9 +81,15 @@ def _grid(g) -> np.ndarray:
     return np.ascontiguousarray(a)
 
 
+# bhn_brick_trace_config.coeff_layout
+BRICK_F64X11, BRICK_F32X12, BRICK_F64X12 = 0, 1, 2
+
+
 class DeviceBricks:
-    """A ``CoefficientBrickGrid`` checked and uploaded once: float64
-    coefficients and grids on the device, for repeated renders."""
+    """A ``CoefficientBrickGrid`` checked and uploaded once, for repeated
+    renders: float64 grids, and the coefficients as 12-wide cell records (the
+    11 channels and a pad, 16-byte aligned) in float32 for a float16 / float32
+    brick, else float64 -- the renderer interpolates in float64 either way."""
 
     def __init__(self, bricks, device: torch.device | None = None):
         coeffs = np.asarray(bricks.coeffs)
@@ -94,10 +101,12 @@ class DeviceBricks:
             raise ValueError("coefficient brick contains non-finite values")
         self.device = device or dev.require_cuda()
         self.grids = [torch.as_tensor(g, device=self.device) for g in host_grids]
-        # uploaded in the brick's own dtype and widened to float64 on the device (exact)
+        # uploaded in the brick's own dtype, padded to records on the device (widening is exact)
         src = np.ascontiguousarray(coeffs if coeffs.dtype in (np.float16, np.float32, np.float64) else
                                    coeffs.astype(np.float64))
-        self.coeffs = torch.from_numpy(src).to(self.device).to(torch.float64)
+        wide = torch.float64 if src.dtype == np.float64 else torch.float32
+        self.layout = BRICK_F64X12 if wide == torch.float64 else BRICK_F32X12
+        self.records = torch.nn.functional.pad(torch.from_numpy(src).to(self.device).to(wide), (0, 1)).contiguous()
 
 
 def _view_and_config(cfg, snapshot, tile, full_trace=False):
@@ -159,9 +168,14 @@ def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagn
     out = torch.empty((h, w, 4), dtype=torch.float64, device=device)
     diag = torch.empty((h, w, 4), dtype=torch.float64, device=device) if diagnostics else None
     g, n = bricks.grids, bricks.shape
-    _lib.check(L.bhn_brick_trace_render(dev.ptr(bricks.coeffs), dev.ptr(g[0]), n[0], dev.ptr(g[1]), n[1], dev.ptr(g[2]),
+    c.coeff_layout = bricks.layout
+    _lib.check(L.bhn_brick_trace_render(dev.ptr(bricks.records), dev.ptr(g[0]), n[0], dev.ptr(g[1]), n[1], dev.ptr(g[2]),
                                         n[2], ctypes.byref(v), ctypes.byref(c), sp, nbytes, dev.ptr(out),
                                         dev.ptr(diag), dev.stream_ptr()))
+    # word 5 of the scratch (bhn_render_prepare's queue state): bit 0 set when the two-warp form of the
+    # renderer gave up a wait between its geodesic and transfer warps (a fault, never a slow image)
+    if int(scratch.view(torch.int32)[(sp - dev.ptr(scratch)) // 4 + 5].item()) & 1:
+        raise RuntimeError("brick renderer: a wait between the geodesic and transfer warps timed out")
     return (out, diag) if diagnostics else out
 
 

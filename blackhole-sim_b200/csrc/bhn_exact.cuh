@@ -94,6 +94,7 @@ __device__ __forceinline__ bool lerp_cells(const double *__restrict__ coeffs, in
 struct AxisHints {
     int kind[3];
     double off[3], inv[3];
+    double g0[3], gn[3];  // first and last knot
 };
 
 __device__ __forceinline__ void classify_axis_warp(const double *g, int n, int lane, int &kind, double &off,
@@ -136,47 +137,132 @@ __device__ __forceinline__ void load_axis_hints(AxisHints &h, const double *rg, 
                                inv);
             if (!(isfinite(off) && isfinite(inv))) kind = kSearch;
             if (lane == 0) {
+                const double *g = a == 0 ? rg : (a == 1 ? tg : pg);
+                const int n = a == 0 ? nr : (a == 1 ? nt : np);
                 h.kind[a] = kind;
                 h.off[a] = off;
                 h.inv[a] = inv;
+                h.g0[a] = g[0];
+                h.gn[a] = g[n - 1];
             }
         }
     }
     __syncthreads();
 }
 
-// bracket_linear_exact with the cell found from the axis hint: the guess is
-// clamped and then fixed up against the knots, which gives
-// searchsorted(side="right") - 1 exactly for any sorted grid.
+// The cell of x (g0 <= x < gn) on an axis: largest i in [0, n-2] with
+// g[i] <= x, as locate_linear, returned with g[i] and g[i+1].  On a classified
+// axis (uniform or geometric: the closed-form guess is within one cell, see
+// locate_linear_f) the guess's neighbours are loaded at once and the fix-up is
+// a select; a guess found off by more (never on a classified axis) falls back
+// to stepping.
+__device__ __forceinline__ int locate_linear_sel(const double *g, int n, double x, int kind, double off, double inv,
+                                                 double &gl, double &gh) {
+    int i;
+    if (kind == kSearch) {
+        i = max(0, min(search_right(g, 0, n, x) - 1, n - 2));
+    } else {
+        const float f = kind == kUniform ? (float)fma(x, inv, -off) : fmaf(__logf((float)x), (float)inv, -(float)off);
+        i = max(0, min((int)fmaxf(f, 0.0f), n - 2));
+        const double gm = g[max(i - 1, 0)], gi = g[i], gi1 = g[i + 1], gp = g[min(i + 2, n - 1)];
+        if (i > 0 && x < gi) {
+            --i;
+            gl = gm;
+            gh = gi;
+        } else if (i < n - 2 && x >= gi1) {
+            ++i;
+            gl = gi1;
+            gh = gp;
+        } else {
+            gl = gi;
+            gh = gi1;
+        }
+        if ((i == 0 || x >= gl) && (i == n - 2 || x < gh)) return i;
+        while (i > 0 && x < g[i]) --i;
+        while (i < n - 2 && x >= g[i + 1]) ++i;
+    }
+    gl = g[i];
+    gh = g[i + 1];
+    return i;
+}
+
+// The phi cell of the wrapped p >= g0: largest i in [0, n-1] with g[i] <= p,
+// as locate_phi, returned with g[i] (the same select form).
+__device__ __forceinline__ int locate_phi_sel(const double *g, int n, double p, int kind, double off, double inv,
+                                              double &gl) {
+    int i;
+    if (kind == kSearch) {
+        i = max(0, min(search_right(g, 0, n, p) - 1, n - 1));
+    } else {
+        i = max(0, min((int)fmaxf((float)fma(p, inv, -off), 0.0f), n - 1));
+        const double gm = g[max(i - 1, 0)], gi = g[i], gi1 = g[min(i + 1, n - 1)], gp = g[min(i + 2, n - 1)];
+        double gnext;
+        if (i > 0 && p < gi) {
+            --i;
+            gl = gm;
+            gnext = gi;
+        } else if (i < n - 1 && p >= gi1) {
+            ++i;
+            gl = gi1;
+            gnext = gp;
+        } else {
+            gl = gi;
+            gnext = gi1;
+        }
+        if ((i == 0 || p >= gl) && (i == n - 1 || p < gnext)) return i;
+        while (i > 0 && p < g[i]) --i;
+        while (i < n - 1 && p >= g[i + 1]) ++i;
+    }
+    gl = g[i];
+    return i;
+}
+
+// bracket_linear_exact with the cell found from the axis hint: the same cell
+// (searchsorted(side="right") - 1) and the same weight for any sorted grid.
 __device__ __forceinline__ bool bracket_linear_hinted(const double *g, int n, double x, int kind, double off,
-                                                      double inv, int &i0, double &w) {
-    if (x < g[0] || x > g[n - 1]) return false;
-    if (x == g[n - 1]) {
+                                                      double inv, double g0, double gn, int &i0, double &w) {
+    if (x < g0 || x > gn) return false;
+    if (x == gn) {
         i0 = n - 2;
         w = 1.0;
         return true;
     }
-    const int lo = x == x ? locate_linear(g, n, x, kind, off, inv) : n - 2;  // NaN: the search's answer
-    double den = sub(g[lo + 1], g[lo]);
+    double gl, gh;
+    int lo;
+    if (x == x) {
+        lo = locate_linear_sel(g, n, x, kind, off, inv, gl, gh);
+    } else {  // NaN: the search's answer
+        lo = n - 2;
+        gl = g[n - 2];
+        gh = gn;
+    }
+    double den = sub(gh, gl);
     if (den < 1.0e-300) den = 1.0e-300;
     i0 = lo;
-    w = sub(x, g[lo]) / den;
+    w = sub(x, gl) / den;
     return true;
 }
 
 // bracket_phi_exact with the hinted cell search.
 __device__ __forceinline__ void bracket_phi_hinted(const double *g, int n, double phi, int kind, double off,
-                                                   double inv, int &i0, int &i1, double &w) {
-    double p = wrap_phi(phi, g[0]);
-    const int lo = (p >= g[0]) ? locate_phi(g, n, p, kind, off, inv) : n - 1;  // below g0 or NaN: the search's answer
+                                                   double inv, double g0, int &i0, int &i1, double &w) {
+    double p = wrap_phi(phi, g0);
+    double gl;
+    int lo;
+    if (p >= g0) {
+        lo = locate_phi_sel(g, n, p, kind, off, inv, gl);
+    } else {  // below g0 or NaN: the search's answer
+        lo = n - 1;
+        gl = g[n - 1];
+    }
     int hi_i = (lo + 1) % n;
-    double hi = hi_i > lo ? g[hi_i] : add(g[0], kTwoPi);
-    double pp = p >= g[lo] ? p : add(p, kTwoPi);
-    double den = sub(hi, g[lo]);
+    double hi = hi_i > lo ? g[hi_i] : add(g0, kTwoPi);
+    double pp = p >= gl ? p : add(p, kTwoPi);
+    double den = sub(hi, gl);
     if (den < 1.0e-300) den = 1.0e-300;
     i0 = lo;
     i1 = hi_i;
-    w = sub(pp, g[lo]) / den;
+    w = sub(pp, gl) / den;
 }
 
 // lib.rs:171-208 / native_kernels.py:164-186
@@ -196,11 +282,100 @@ __device__ __forceinline__ bool sample_one_hinted(const double *__restrict__ coe
                                                   const AxisHints &h, double r, double th, double ph, double out[11]) {
     int r0, t0, p0, p1;
     double wr, wt, wp;
-    if (!bracket_linear_hinted(rg, nr, r, h.kind[0], h.off[0], h.inv[0], r0, wr) ||
-        !bracket_linear_hinted(tg, nt, th, h.kind[1], h.off[1], h.inv[1], t0, wt))
+    if (!bracket_linear_hinted(rg, nr, r, h.kind[0], h.off[0], h.inv[0], h.g0[0], h.gn[0], r0, wr) ||
+        !bracket_linear_hinted(tg, nt, th, h.kind[1], h.off[1], h.inv[1], h.g0[1], h.gn[1], t0, wt))
         return false;
-    bracket_phi_hinted(pg, np, ph, h.kind[2], h.off[2], h.inv[2], p0, p1, wp);
+    bracket_phi_hinted(pg, np, ph, h.kind[2], h.off[2], h.inv[2], h.g0[2], p0, p1, wp);
     return lerp_cells(coeffs, nt, np, r0, t0, p0, p1, wr, wt, wp, out);
+}
+
+// Cell records: the 11 channels of a cell and one pad, 16-byte aligned, in
+// float32 (a float32 brick, 48 B, three 128-bit loads per cell) or float64
+// (96 B, six).  A ray's eight corners sit at scattered addresses, so each warp
+// load costs about one L1 wavefront per lane; 128-bit records cut the loads of
+// a float32 brick's sample from 88 to 24.
+template <typename T>
+struct RecordVec;
+template <>
+struct RecordVec<float> {
+    using V = float4;
+    static constexpr int n = 4;
+    __device__ static void widen(const float4 &v, double o[4]) {
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+    }
+};
+template <>
+struct RecordVec<double> {
+    using V = double2;
+    static constexpr int n = 2;
+    __device__ static void widen(const double2 &v, double o[2]) {
+        o[0] = v.x;
+        o[1] = v.y;
+    }
+};
+
+// The trilinear value of the 11 channels from the eight corner weights
+// (products of the per-axis weights, formed once) and one fused multiply-add
+// per corner and channel: 100 float64 operations instead of lerp_cells' 231
+// separately rounded ones, equal to them within a few ulps.  Layout picks the
+// corner loads: the [..][11] float64 brick (scalar loads) or 12-wide cell
+// records in float32 / float64 (128-bit loads, values widened exactly).
+template <typename T, int Stride>
+__device__ __forceinline__ void lerp_weighted(const T *__restrict__ cells, int nt, int np, int r0, int t0, int p0,
+                                              int p1, double wr, double wt, double wp, double out[11]) {
+    const int r1 = r0 + 1, t1 = t0 + 1;
+    auto cell = [&](int ir, int it, int ip) { return cells + ((((int64_t)ir * nt + it) * np) + ip) * Stride; };
+    const T *q[8] = {cell(r0, t0, p0), cell(r0, t0, p1), cell(r0, t1, p0), cell(r0, t1, p1),
+                     cell(r1, t0, p0), cell(r1, t0, p1), cell(r1, t1, p0), cell(r1, t1, p1)};
+    const double owp = 1.0 - wp, owt = 1.0 - wt, owr = 1.0 - wr;
+    const double a00 = owr * owt, a01 = owr * wt, a10 = wr * owt, a11 = wr * wt;
+    const double w[8] = {a00 * owp, a00 * wp, a01 * owp, a01 * wp, a10 * owp, a10 * wp, a11 * owp, a11 * wp};
+    if constexpr (Stride == 12) {
+        using RV = RecordVec<T>;
+        constexpr int W = RV::n;
+#pragma unroll
+        for (int g = 0; g < 12 / W; ++g) {
+            double acc[W];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                double v[W];
+                RV::widen(__ldg(reinterpret_cast<const typename RV::V *>(q[k]) + g), v);
+#pragma unroll
+                for (int j = 0; j < W; ++j) acc[j] = k == 0 ? w[0] * v[j] : fma(w[k], v[j], acc[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < W; ++j)
+                if (g * W + j < 11) out[g * W + j] = acc[j];
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 11; ++c) {
+            double acc = w[0] * __ldg(q[0] + c);
+#pragma unroll
+            for (int k = 1; k < 8; ++k) acc = fma(w[k], __ldg(q[k] + c), acc);
+            out[c] = acc;
+        }
+    }
+}
+
+// sample_one_hinted's cells and per-axis weights, blended by lerp_weighted
+// over the [..][Stride] cells (Stride 11: the reference's layout; 12: records).
+template <typename T, int Stride>
+__device__ __forceinline__ bool sample_weighted_hinted(const T *__restrict__ rec, const double *rg, int nr,
+                                                      const double *tg, int nt, const double *pg, int np,
+                                                      const AxisHints &h, double r, double th, double ph,
+                                                      double out[11]) {
+    int r0, t0, p0, p1;
+    double wr, wt, wp;
+    if (!bracket_linear_hinted(rg, nr, r, h.kind[0], h.off[0], h.inv[0], h.g0[0], h.gn[0], r0, wr) ||
+        !bracket_linear_hinted(tg, nt, th, h.kind[1], h.off[1], h.inv[1], h.g0[1], h.gn[1], t0, wt))
+        return false;
+    bracket_phi_hinted(pg, np, ph, h.kind[2], h.off[2], h.inv[2], h.g0[2], p0, p1, wp);
+    lerp_weighted<T, Stride>(rec, nt, np, r0, t0, p0, p1, wr, wt, wp, out);
+    return true;
 }
 
 }  // namespace bhn

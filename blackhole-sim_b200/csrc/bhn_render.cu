@@ -150,6 +150,7 @@ __global__ void setup_views_kernel(const bhn_view *__restrict__ raw, int n, View
         axis_begin[n] = acc_axis;
         q->total = (unsigned long long)acc;
         q->n_views = (uint32_t)n;
+        q->error_flags = 0;  // bit 0: the brick renderer's two-warp form gave up a wait
     }
 }
 

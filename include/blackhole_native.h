@@ -412,8 +412,13 @@ int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, cons
  * nonperiodic r / theta range), ds = length_cm * max(|d(r, theta, phi)|,
  * 1e-14), an RK2 or exact Stokes step, the optical-depth cutoff, and
  * non-finite results set to 0; FP64, one thread per ray.  (bhn_render_launch
- * is the RK2, h = 0.02 r form of the same loop.)  coeffs: [nr][nt][np][11]
- * float64; out: [rays][4] at view->out_offset; diag (optional): [rays][4] =
+ * is the RK2, h = 0.02 r form of the same loop.)  coeffs: per
+ * cfg->coeff_layout, [nr][nt][np][11] float64 (BHN_BRICK_F64X11, the
+ * CoefficientBrickGrid layout) or [nr][nt][np][12] cell records, 11 channels
+ * and one unused pad, 16-byte aligned, in float32 (BHN_BRICK_F32X12: a float32
+ * brick, read with three 128-bit loads per cell) or float64
+ * (BHN_BRICK_F64X12); the interpolation is float64 either way (float32 values
+ * widen exactly), so the three give the same image; out: [rays][4] at view->out_offset; diag (optional): [rays][4] =
  * optical depth, sampled segments, RK4 steps taken, BHN_RAY_* status.
  * Unless full_trace is set, a ray's trace also ends once it is past the
  * brick's outer radius, moving out, with a radial potential that keeps it
@@ -422,6 +427,7 @@ int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, cons
  * same bit for bit, and only the diag columns "RK4 steps taken" and
  * "status" differ from the full trace's.
  * scratch: bhn_render_scratch_bytes(1). */
+enum { BHN_BRICK_F64X11 = 0, BHN_BRICK_F32X12 = 1, BHN_BRICK_F64X12 = 2 };
 typedef struct bhn_brick_trace_config {
     double step;                 /* affine RK4 step (AcceleratedRenderConfig.step) */
     double escape_radius;
@@ -431,8 +437,9 @@ typedef struct bhn_brick_trace_config {
     int32_t exact_step;          /* 1: stokes_step_exact, 0: RK2 */
     int32_t full_trace;          /* 1: trace every ray to the reference's own end (escape radius, capture,
                                     max_steps), 0: also end outbound rays past the brick (same image) */
+    int32_t coeff_layout;        /* BHN_BRICK_*: layout of coeffs */
 } bhn_brick_trace_config;
-int bhn_brick_trace_render(const double *coeffs, const double *r_grid, int32_t nr, const double *theta_grid,
+int bhn_brick_trace_render(const void *coeffs, const double *r_grid, int32_t nr, const double *theta_grid,
                            int32_t nt, const double *phi_grid, int32_t np, const bhn_view *view,
                            const bhn_brick_trace_config *cfg, void *scratch, int64_t scratch_bytes, double *out,
                            double *diag, void *stream);

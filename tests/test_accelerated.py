@@ -172,10 +172,14 @@ def test_c_abi_rejects_bad_arguments_before_device_work():
     assert call(out=None) == 1 and b"missing" in L.bhn_last_error()
     assert call(nr=1) == 1 and b"at least 2" in L.bhn_last_error()
     for field, value, msg in (("step", 0.0, b"step"), ("step", float("nan"), b"step"), ("max_steps", -1, b"max_steps"),
-                              ("length_cm", float("inf"), b"finite")):
+                              ("length_cm", float("inf"), b"finite"), ("coeff_layout", 3, b"layout")):
         bad = acc.BrickTraceConfigStruct.from_buffer_copy(c)
         setattr(bad, field, value)
         assert call(cfg=bad) == 1 and msg in L.bhn_last_error(), field
+    rec = acc.BrickTraceConfigStruct.from_buffer_copy(c)
+    rec.coeff_layout = acc.BRICK_F32X12
+    assert L.bhn_brick_trace_render(p + 8 if p % 16 == 0 else p, p, 4, p, 4, p, 4, ctypes.byref(v), ctypes.byref(rec),
+                                    p, 512, p, None, None) == 1 and b"16-byte" in L.bhn_last_error()
 
 
 def test_config_struct_layout_matches_ctypes(tmp_path):
@@ -190,15 +194,16 @@ def test_config_struct_layout_matches_ctypes(tmp_path):
     include = Path(__file__).resolve().parents[1] / "include"
     src = tmp_path / "sizes.c"
     src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "blackhole_native.h"\n'
-                   'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(bhn_brick_trace_config),'
+                   'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(bhn_brick_trace_config),'
                    ' offsetof(bhn_brick_trace_config, max_steps), offsetof(bhn_brick_trace_config, exact_step),'
-                   ' offsetof(bhn_brick_trace_config, full_trace));'
+                   ' offsetof(bhn_brick_trace_config, full_trace), offsetof(bhn_brick_trace_config, coeff_layout));'
                    ' return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", str(include), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     S = acc.BrickTraceConfigStruct
-    assert got == [ctypes.sizeof(S), S.max_steps.offset, S.exact_step.offset, S.full_trace.offset]
+    assert got == [ctypes.sizeof(S), S.max_steps.offset, S.exact_step.offset, S.full_trace.offset,
+                   S.coeff_layout.offset]
 
 
 @pytest.mark.gpu
@@ -393,3 +398,57 @@ def test_gpu_outbound_exit_keeps_the_image(golden):
         assert torch.all(diag[..., 2] <= rdiag[..., 2]) and not np.any(rst == 5)
         outbound += int(out.sum())
     assert outbound > 0.5 * 160 * 90
+
+
+@pytest.mark.gpu
+def test_gpu_coefficient_layouts_give_one_image(golden):
+    """The brick as the reference holds it ([..][11] float64) and as 12-wide
+    cell records in float32 and float64 give bit-identical images and
+    diagnostics: the records only change how the corners are loaded."""
+    import torch
+
+    from blackhole_native import accelerated as acc
+
+    snap = SimpleNamespace(spin_a=0.9375)
+    cfg = _config(acc, golden["acc_cam"], "rk2", "full")
+    cfg = acc.AcceleratedRenderConfig(width=24, height=16, camera=cfg.camera, step=0.1, max_steps=900,
+                                      transfer=cfg.transfer)
+    db = acc.DeviceBricks(_golden_bricks(golden, np.float32))
+    assert db.layout == acc.BRICK_F32X12 and db.records.shape[-1] == 12 and db.records.data_ptr() % 16 == 0
+    ref = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True)
+    wide = db.records[..., :11].to(torch.float64).contiguous()
+    for layout, rec in ((acc.BRICK_F64X11, wide),
+                        (acc.BRICK_F64X12, torch.nn.functional.pad(wide, (0, 1)).contiguous())):
+        db.records, db.layout = rec, layout
+        got = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True)
+        assert torch.equal(got[0], ref[0]) and torch.equal(got[1], ref[1]), layout
+    d64 = acc.DeviceBricks(_golden_bricks(golden, np.float64))
+    assert d64.layout == acc.BRICK_F64X12
+
+
+@pytest.mark.gpu
+def test_gpu_one_and_two_warp_forms_agree(golden):
+    """An image with more warps than 8 per SM runs the one-warp kernel; its
+    tiles, small enough for the two-warp form (geodesic warp + transfer warp
+    per 32 rays), must give the same pixels and diagnostics bit for bit."""
+    import torch
+
+    from blackhole_native import accelerated as acc
+    from blackhole_native.tiles import RenderTile
+
+    snap = SimpleNamespace(spin_a=0.9375)
+    base = _config(acc, golden["acc_cam"], "rk2", "cut")
+    cfg = acc.AcceleratedRenderConfig(width=256, height=160, camera=base.camera, step=0.1, max_steps=900,
+                                      transfer=base.transfer)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert 256 * 160 // 32 > 8 * sms and 128 * 80 // 32 <= 8 * sms
+    db = acc.DeviceBricks(_golden_bricks(golden))
+    img, diag = acc.render_stokes_image_bricks_device(cfg, snap, db, diagnostics=True)
+    for y0 in (0, 80):
+        for x0 in (0, 128):
+            t = RenderTile(level=0, y0=y0, x0=x0, x1=x0 + 128, y1=y0 + 80)
+            ti, td = acc.render_stokes_image_bricks_device(cfg, snap, db, tile=t, diagnostics=True)
+            assert torch.equal(ti, img[y0:y0 + 80, x0:x0 + 128]), (x0, y0)
+            assert torch.equal(td, diag[y0:y0 + 80, x0:x0 + 128]), (x0, y0)
+    st = diag[..., 3].cpu().numpy()
+    assert np.any(st == 4) and np.any(st == 5)  # the cutoff and the outbound exit both occur
