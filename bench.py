@@ -1003,16 +1003,19 @@ def bench_bricks(args) -> dict | None:
     time.sleep(0.3)
     barrier(world)
     outs = []
-    per = timed_launches(lambda: outs.append(acc.render_stokes_image_bricks_device(cfg, snap, db)), args.steps,
-                         stream, device)
+    # unchecked launches (no read-back inside the timed region); every image is compared with the checked one below
+    per = timed_launches(lambda: outs.append(acc.render_stokes_image_bricks_device(cfg, snap, db, check=False)),
+                         args.steps, stream, device)
     barrier(world)
     clk = clocks.stop()
     assert all(torch.equal(o, img) for o in outs), "images differ between launches"
     t_max = max_over_ranks(sum(per), world, device)
     value = sum_over_ranks(pixels * args.steps, world, device) / (t_max * 1e-3)
     # the same image with every ray traced to the reference's own end (escape radius 220, capture, max_steps)
-    per_full = timed_launches(lambda: acc.render_stokes_image_bricks_device(cfg, snap, db, full_trace=True),
-                              args.steps, stream, device)
+    full_outs = []
+    per_full = timed_launches(lambda: full_outs.append(acc.render_stokes_image_bricks_device(
+        cfg, snap, db, full_trace=True, check=False)), args.steps, stream, device)
+    assert all(torch.equal(o, img) for o in full_outs), "full-trace images differ
     full_trace = {"ms_per_step": statistics.mean(per_full), "pixels_per_s": pixels / (statistics.mean(per_full) * 1e-3),
                   "rk4_steps_per_step": float(fd[..., 2].sum()), "longest_ray_steps": int(fd[..., 2].max()),
                   "note": "full_trace=True: rays also traced past the brick to the escape radius; same image"}
@@ -1066,7 +1069,7 @@ def bench_bricks(args) -> dict | None:
                      "algorithmic_flops_per_launch": flops,
                      "flop_per_rk4_step": FP64_FLOP_PER_RK4_STEP, "flop_per_segment": FP64_FLOP_PER_SEGMENT},
         "cpu_baseline": cpu,
-        "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per)},
+        "kernel_ms": {"mean": per_mean, "min": min(per), "max": max(per), "all": [round(x, 3) for x in per]},
         "full_trace": full_trace,
     }
     if world > 1:

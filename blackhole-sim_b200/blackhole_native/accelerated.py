@@ -141,7 +141,8 @@ def _view_and_config(cfg, snapshot, tile, full_trace=False):
 
 
 def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagnostics: bool = False,
-                                      device: torch.device | None = None, full_trace: bool = False):
+                                      device: torch.device | None = None, full_trace: bool = False,
+                                      check: bool = True):
     """(h, w, 4) float64 Stokes image of the tile (default: the whole image)
     on the device, and (h, w, 4) diagnostics (columns ``DIAGNOSTICS``) when
     asked.  ``snapshot`` supplies the spin (``spin_a``); ``bricks`` is a
@@ -152,7 +153,11 @@ def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagn
     ``full_trace`` -- once it is past the brick's outer radius moving out with
     no radial turning point ahead (status ``outbound``): nothing after either
     cutoff is sampled, so the image is the same; only the diagnostics' step
-    count and status differ from a full trace's."""
+    count and status differ from a full trace's.
+
+    ``check`` reads the launch's error word back (a synchronising 4-byte
+    copy) and raises if the renderer gave up a wait; unchecked, such a launch
+    leaves NaN in the rays it did not finish."""
     # host-side checks first: a bad call fails the same way with or without a GPU
     v, c, (h, w) = _view_and_config(cfg, snapshot, tile, full_trace)
     if not isinstance(bricks, DeviceBricks):
@@ -174,7 +179,7 @@ def render_stokes_image_bricks_device(cfg, snapshot, bricks, *, tile=None, diagn
                                         dev.ptr(diag), dev.stream_ptr()))
     # word 5 of the scratch (bhn_render_prepare's queue state): bit 0 set when the two-warp form of the
     # renderer gave up a wait between its geodesic and transfer warps (a fault, never a slow image)
-    if int(scratch.view(torch.int32)[(sp - dev.ptr(scratch)) // 4 + 5].item()) & 1:
+    if check and int(scratch.view(torch.int32)[(sp - dev.ptr(scratch)) // 4 + 5].item()) & 1:
         raise RuntimeError("brick renderer: a wait between the geodesic and transfer warps timed out")
     return (out, diag) if diagnostics else out
 
