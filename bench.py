@@ -1015,7 +1015,7 @@ def bench_bricks(args) -> dict | None:
     full_outs = []
     per_full = timed_launches(lambda: full_outs.append(acc.render_stokes_image_bricks_device(
         cfg, snap, db, full_trace=True, check=False)), args.steps, stream, device)
-    assert all(torch.equal(o, img) for o in full_outs), "full-trace images differ
+    assert all(torch.equal(o, img) for o in full_outs), "full-trace images differ"
     full_trace = {"ms_per_step": statistics.mean(per_full), "pixels_per_s": pixels / (statistics.mean(per_full) * 1e-3),
                   "rk4_steps_per_step": float(fd[..., 2].sum()), "longest_ray_steps": int(fd[..., 2].max()),
                   "note": "full_trace=True: rays also traced past the brick to the escape radius; same image"}
@@ -1064,8 +1064,10 @@ def bench_bricks(args) -> dict | None:
         "roofline": {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(peaks["fma_tflops"], 2),
                      "unit": "TFLOP/s", "frac": round(achieved / peaks["fma_tflops"], 4),
                      "traffic": profiled_traffic(BRICKS_PROFILE),
+                     "traffic_source": f"ncu capture of the same workload ({BRICKS_PROFILE.relative_to(REPO)})",
                      "peak_source": "measured in this run (bhn_fp64_peak_probe FMA chains)",
-                     "kernel": "brick_trace_kernel",
+                     "kernel": ("brick_trace_pair_kernel" if (pixels + 31) // 32 <= 8 * torch.cuda.get_device_properties(
+                         device).multi_processor_count else "brick_trace_kernel"),
                      "algorithmic_flops_per_launch": flops,
                      "flop_per_rk4_step": FP64_FLOP_PER_RK4_STEP, "flop_per_segment": FP64_FLOP_PER_SEGMENT},
         "cpu_baseline": cpu,
