@@ -148,6 +148,7 @@ class GrrtConfigStruct(ctypes.Structure):
         ("flux_scale", ctypes.c_double),
         ("max_steps", ctypes.c_int32),
         ("exact_step", ctypes.c_int32),
+        ("full_trace", ctypes.c_int32),
     ]
 
 
@@ -219,12 +220,16 @@ def default_chunk(rays: int) -> int:
 
 def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diagnostics: bool = False,
                                device: torch.device | None = None, out: torch.Tensor | None = None,
-                               chunk: int | None = None):
+                               chunk: int | None = None, full_trace: bool = False):
     """(H, W, 4) float64 Stokes image on the device (and (H, W, 8) diagnostics,
     columns ``DIAGNOSTICS``, when asked).  ``snapshot`` is a host snapshot or a
     ``DeviceSnapshot``; ``out`` an optional preallocated (H, W, 4) float64
     device tensor; ``chunk`` the emitting segments listed per ray and round
-    (memory against rounds; the image does not depend on it)."""
+    (memory against rounds; the image does not depend on it).  Unless
+    ``full_trace``, a ray past the snapshot's outer radius moving out with no
+    radial turning point ahead ends there (status 5, outbound): no later
+    segment lies in the snapshot, so the image is the same and only the
+    diagnostics' step count and status differ from a full trace's."""
     L = _declare()
     ds = snapshot if isinstance(snapshot, DeviceSnapshot) else DeviceSnapshot(snapshot, device)
     device = ds.device
@@ -244,6 +249,7 @@ def render_stokes_image_device(cfg, snapshot, scaling, *, coeff_model=None, diag
     c.length_cm, c.max_optical_depth, c.min_redshift = _length_cm(t, scaling), float(t.max_optical_depth), float(t.min_redshift)
     c.flux_scale = float(getattr(scaling, "flux_scale_jy", 1.0))
     c.max_steps, c.exact_step = int(cfg.max_steps), int(bool(t.use_exact_matrix_step))
+    c.full_trace = int(bool(full_trace))
     m = model_struct(coeff_model or HybridSynchrotronCoefficients(), t.observing_frequency_hz, scaling)
     rays = v.width * v.height
     chunk = default_chunk(rays) if chunk is None else int(chunk)

@@ -17,39 +17,6 @@
 
 namespace bhn {
 
-// Whether a ray at radius r, moving out (p_r > 0), keeps moving out for good.
-// With E = -p_t, L = p_phi, the state's own 2H = g^{mu nu} p_mu p_nu (the
-// fixed-step integrator's drift from the null value 0, up to ~1e-3 E^2 after
-// a pass near the hole) and the Carter constant of that H,
-// K = p_theta^2 + (L / sin - a E sin)^2 - 2H a^2 cos^2, the radial motion obeys
-// (Delta p_r)^2 = R(r) = (E (r^2 + a^2) - a L)^2 - Delta (K - 2H r^2)
-//                     = (E^2 + 2H) r^4 - 4H r^3 + c2 r^2 + 2K r + c0,
-// c2 = 2 E B - K + 2H a^2, c0 = B^2 - a^2 K, B = a (a E - L).  For every
-// r' >= r (K >= 0; r'^3 <= r'^4 / r), R(r') >= e r'^4 + c2 r'^2 + c0 with
-// e = E^2 - |2H| (1 + 2 / r), and that is >= e r'^4 / 4 when
-// g(u) = 3/4 e u^2 + c2 u + c0 and g'(u) are >= 0 at u = r^2 (g increases
-// beyond).  R then never vanishes, so r never turns; the factor-4 margin
-// dwarfs the RK4 truncation this far out.
-__device__ __forceinline__ bool outbound_for_good(double r, double th, double pr, double pth, double pt,
-                                                  double pphi, double a) {
-    const double E = -pt, L = pphi;
-    if (!(pr > 0.0) || !(E > 0.0)) return false;
-    double s, c;
-    sincos(safe_theta(th), &s, &c);
-    const double w = L / s - a * E * s;
-    const double u = r * r, a2 = a * a, cc = c * c;
-    const double dlt = u - 2.0 * r + a2, sig = u + a2 * cc;
-    const double P = E * (u + a2) - a * L;
-    const double k0 = pth * pth + w * w;
-    const double h2 = (dlt * pr * pr + k0 - P * P / dlt) / sig;  // 2H
-    const double K = k0 - h2 * a2 * cc;
-    const double e = E * E - fabs(h2) * (1.0 + 2.0 / r);
-    if (!(K >= 0.0) || !(e > 0.0)) return false;
-    const double B = a * (a * E - L);
-    const double e2 = 0.75 * e, c2 = 2.0 * E * B - K + h2 * a2, c0 = B * B - a2 * K;
-    return (2.0 * e2 * u + c2 >= 0.0) && ((e2 * u + c2) * u + c0 >= 0.0);
-}
-
 struct BrickTraceParams {
     const void *coeffs;          // [nr][nt][np][11] float64, or 12-wide cell records (BHN_BRICK_*)
     const double *rg, *tg, *pg;

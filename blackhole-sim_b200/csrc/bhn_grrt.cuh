@@ -66,6 +66,7 @@ struct TraceParams {
     int nr, nt, np, max_steps;
     const ViewDev *view;
     double step, escape_radius, nu, length_cm, min_redshift, flux_scale, rho_unit, b_unit, mu_e_mp;
+    int full_trace;             // 0: a ray past the snapshot's outer radius, moving out for good, ends there
     WaveState W;
 };
 struct CoefParams {
@@ -80,6 +81,39 @@ struct TransferParams {
     double *diag;               // optional [rays][8]: tau, emit, valid, faraday depth, g min, g max, steps, status
     WaveState W;
 };
+
+// Whether a ray at radius r, moving out (p_r > 0), keeps moving out for good.
+// With E = -p_t, L = p_phi, the state's own 2H = g^{mu nu} p_mu p_nu (the
+// fixed-step integrator's drift from the null value 0, up to ~1e-3 E^2 after
+// a pass near the hole) and the Carter constant of that H,
+// K = p_theta^2 + (L / sin - a E sin)^2 - 2H a^2 cos^2, the radial motion obeys
+// (Delta p_r)^2 = R(r) = (E (r^2 + a^2) - a L)^2 - Delta (K - 2H r^2)
+//                     = (E^2 + 2H) r^4 - 4H r^3 + c2 r^2 + 2K r + c0,
+// c2 = 2 E B - K + 2H a^2, c0 = B^2 - a^2 K, B = a (a E - L).  For every
+// r' >= r (K >= 0; r'^3 <= r'^4 / r), R(r') >= e r'^4 + c2 r'^2 + c0 with
+// e = E^2 - |2H| (1 + 2 / r), and that is >= e r'^4 / 4 when
+// g(u) = 3/4 e u^2 + c2 u + c0 and g'(u) are >= 0 at u = r^2 (g increases
+// beyond).  R then never vanishes, so r never turns; the factor-4 margin
+// dwarfs the RK4 truncation this far out.
+__device__ __forceinline__ bool outbound_for_good(double r, double th, double pr, double pth, double pt,
+                                                  double pphi, double a) {
+    const double E = -pt, L = pphi;
+    if (!(pr > 0.0) || !(E > 0.0)) return false;
+    double s, c;
+    sincos(safe_theta(th), &s, &c);
+    const double w = L / s - a * E * s;
+    const double u = r * r, a2 = a * a, cc = c * c;
+    const double dlt = u - 2.0 * r + a2, sig = u + a2 * cc;
+    const double P = E * (u + a2) - a * L;
+    const double k0 = pth * pth + w * w;
+    const double h2 = (dlt * pr * pr + k0 - P * P / dlt) / sig;  // 2H
+    const double K = k0 - h2 * a2 * cc;
+    const double e = E * E - fabs(h2) * (1.0 + 2.0 / r);
+    if (!(K >= 0.0) || !(e > 0.0)) return false;
+    const double B = a * (a * E - L);
+    const double e2 = 0.75 * e, c2 = 2.0 * E * B - K + h2 * a2, c0 = B * B - a2 * K;
+    return (2.0 * e2 * u + c2 >= 0.0) && ((e2 * u + c2) * u + c0 >= 0.0);
+}
 
 __device__ __forceinline__ void rk4_state(const double y[5], double h, double a, double pt, double pphi, double yn[5]) {
     // kerr.py:306-313 on (r, theta, phi, p_r, p_theta)
@@ -151,6 +185,7 @@ __global__ void __launch_bounds__(128) grrt_trace_kernel(const TraceParams P) {
     if (R.status >= 0 || R.trace_status >= 0) return;
     const ViewDev &v = *P.view;
     const double a = v.a, pt = R.pt, pphi = R.pphi;
+    const double r_edge = P.full_trace ? INFINITY : fmax(hints.g0[0], hints.gn[0]);
     double y[5] = {R.y[0], R.y[1], R.y[2], R.y[3], R.y[4]};
     double prev_r = R.prev_r;
     int steps = R.steps, valid = R.valid, count = 0, ts = -1;
@@ -224,6 +259,11 @@ __global__ void __launch_bounds__(128) grrt_trace_kernel(const TraceParams P) {
             break;
         }
         prev_r = y[0];
+        // past the snapshot's outer radius for good: every later midpoint lies outside it (no segment)
+        if (y[0] > r_edge && outbound_for_good(y[0], y[1], y[3], y[4], pt, pphi, a)) {
+            ts = BHN_RAY_OUTBOUND;
+            break;
+        }
         if (count == P.W.chunk) break;  // this round's list is full: continue in the next round
     }
     for (int k = 0; k < 5; ++k) R.y[k] = y[k];
@@ -381,6 +421,7 @@ extern "C" int bhn_grrt_render(const double *fields, const double *r_grid, int32
     T.nt = nt;
     T.np = np;
     T.max_steps = cfg->max_steps;
+    T.full_trace = cfg->full_trace != 0;
     T.view = vd;
     T.step = cfg->step;
     T.escape_radius = cfg->escape_radius;

@@ -37,9 +37,9 @@ typedef enum bhn_status {
 enum { BHN_POLICY_NAN = 0, BHN_POLICY_INITIAL = 1, BHN_POLICY_ZERO = 2 };
 
 /* Ray termination status (kerr.py:25 plus the optical-depth cutoff of
- * accelerated_renderer.py:123-125).  BHN_RAY_OUTBOUND (brick renderer only):
- * the ray is past the brick's outer radius, moving out, and can never turn
- * back, so no later segment is sampled and its image is final. */
+ * accelerated_renderer.py:123-125).  BHN_RAY_OUTBOUND (brick and GRRT renderers):
+ * the ray is past the brick's (or snapshot's) outer radius, moving out, and
+ * can never turn back, so no later segment is sampled and its image is final. */
 enum {
     BHN_RAY_MAX_STEPS = 0,
     BHN_RAY_CAPTURED = 1,
@@ -396,6 +396,8 @@ typedef struct bhn_grrt_config {
     double max_optical_depth, min_redshift, flux_scale;
     int32_t max_steps;
     int32_t exact_step;          /* 1: stokes_step_exact, 0: RK2 (PolarizedTransferConfig.use_exact_matrix_step) */
+    int32_t full_trace;          /* 1: trace every ray to the reference's own end; 0: also end a ray past the
+                                    snapshot's outer radius moving out for good (BHN_RAY_OUTBOUND, same image) */
 } bhn_grrt_config;
 int64_t bhn_grrt_scratch_bytes(int64_t rays, int32_t chunk);
 int bhn_grrt_render(const double *fields, const double *r_grid, int32_t nr, const double *theta_grid, int32_t nt,

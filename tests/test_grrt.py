@@ -220,3 +220,34 @@ def test_stokes_to_rgb_and_npz_match_the_reference(tmp_path):
     with np.load(out) as z:
         assert list(z.keys()) == ["stokes"] and z["stokes"].dtype == np.float64
         assert np.array_equal(z["stokes"], g["rgb_in"].astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.gpu
+def test_gpu_outbound_exit_keeps_the_image(golden):
+    """A ray past the snapshot's outer radius moving out for good ends there
+    (status 5): the image and the optical-depth, segment and redshift columns
+    equal a full trace's bit for bit, on the golden scene (with and without a
+    cutoff that ends rays) and on a seeded 32 x 16 x 32 snapshot seen from
+    r = 55 M; outbound rays are ones the full trace ends as escaped or at
+    max_steps, after no more steps."""
+    from blackhole_native import grrt
+
+    sc = _scaling(golden)
+    seeded = grrt.seeded_snapshot(32, 16, 32, 0.9375, 3)
+    scenes = []
+    for max_tau in (30.0, 1e-6):
+        tr = grrt.PolarizedTransferConfig(max_optical_depth=max_tau)
+        scenes.append((grrt.PolarizedRenderConfig(width=12, height=8, camera=grrt.LocalCamera(*golden["cam"]),
+                                                  step=0.1, max_steps=900, transfer=tr), _snapshot(golden)))
+    scenes.append((grrt.PolarizedRenderConfig(width=24, height=14), seeded))
+    outbound = 0
+    for cfg, snap in scenes:
+        img, d = (t.cpu().numpy() for t in grrt.render_stokes_image_device(cfg, snap, sc, diagnostics=True))
+        ref, rd = (t.cpu().numpy() for t in grrt.render_stokes_image_device(cfg, snap, sc, diagnostics=True,
+                                                                           full_trace=True))
+        assert np.array_equal(img, ref) and np.array_equal(d[..., :6], rd[..., :6])
+        out = d[..., 7] == 5
+        assert np.array_equal(d[..., 7][~out], rd[..., 7][~out]) and np.all(np.isin(rd[..., 7][out], (0, 2)))
+        assert np.all(d[..., 6] <= rd[..., 6]) and not np.any(rd[..., 7] == 5)
+        outbound += int(out.sum())
+    assert outbound > 0
