@@ -97,16 +97,19 @@ class DeviceBricks:
         self.shape = tuple(g.size for g in host_grids)
         if coeffs.shape != self.shape + (11,):
             raise ValueError(f"coeffs must have shape {self.shape + (11,)}; got {coeffs.shape}")
-        if not np.all(np.isfinite(coeffs)):
-            raise ValueError("coefficient brick contains non-finite values")
+        if not torch.cuda.is_available() and not np.all(np.isfinite(coeffs)):
+            raise ValueError("coefficient brick contains non-finite values")  # the same error as below, GPU or not
         self.device = device or dev.require_cuda()
-        self.grids = [torch.as_tensor(g, device=self.device) for g in host_grids]
-        # uploaded in the brick's own dtype, padded to records on the device (widening is exact)
+        # uploaded in the brick's own dtype, checked and padded to records on the device (widening is exact)
         src = np.ascontiguousarray(coeffs if coeffs.dtype in (np.float16, np.float32, np.float64) else
                                    coeffs.astype(np.float64))
+        up = torch.from_numpy(src).to(self.device)
+        if not bool(torch.isfinite(up).all()):
+            raise ValueError("coefficient brick contains non-finite values")
+        self.grids = [torch.as_tensor(g, device=self.device) for g in host_grids]
         wide = torch.float64 if src.dtype == np.float64 else torch.float32
         self.layout = BRICK_F64X12 if wide == torch.float64 else BRICK_F32X12
-        self.records = torch.nn.functional.pad(torch.from_numpy(src).to(self.device).to(wide), (0, 1)).contiguous()
+        self.records = torch.nn.functional.pad(up.to(wide), (0, 1)).contiguous()
 
 
 def _view_and_config(cfg, snapshot, tile, full_trace=False):

@@ -123,7 +123,9 @@ def _golden_bricks(golden, dt=np.float32):
 
 
 def test_host_validation_before_any_device_work(golden):
-    """Bad bricks, configs and tiles raise ValueError on the host, GPU or not."""
+    """Bad bricks, configs and tiles raise ValueError, GPU or not: all on the
+    host before any device work, except a non-finite coefficient, which a GPU
+    finds in the uploaded brick (the same error; test_gpu_edge_cases)."""
     from dataclasses import replace
 
     from blackhole_native import accelerated as acc
@@ -217,6 +219,11 @@ def test_gpu_edge_cases(golden):
 
     snap = SimpleNamespace(spin_a=0.9375)
     cfg = _config(acc, golden["acc_cam"], "rk2", "full")
+    nonfinite = _golden_bricks(golden)
+    nonfinite.coeffs = nonfinite.coeffs.copy()
+    nonfinite.coeffs[1, 1, 1, 4] = np.inf
+    with pytest.raises(ValueError, match="non-finite"):
+        acc.render_stokes_image_bricks(cfg, snap, nonfinite)
     img, diag = (t.cpu().numpy() for t in acc.render_stokes_image_bricks_device(
         replace(cfg, max_steps=0), snap, _golden_bricks(golden), diagnostics=True))
     assert not np.any(img) and not np.any(diag[..., :3]) and np.all(diag[..., 3] == 0)  # BHN_RAY_MAX_STEPS
