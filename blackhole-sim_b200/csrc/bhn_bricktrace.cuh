@@ -10,7 +10,11 @@
 // tau += max(alpha_I, 0) ds until tau reaches the cutoff, and the final
 // nan_to_num(nan = posinf = neginf = 0).  Unlike the fused renderer
 // (bhn_render_launch: the RK2 step h = 0.02 r), this is the reference
-// Python's method, one thread per ray.
+// Python's method: one thread per ray (brick_trace_kernel), or, for images of
+// at most 8 ray warps per SM, two warps per 32 rays (brick_trace_pair_kernel:
+// a geodesic warp and a transfer warp joined by an mbarrier ring).  A ray
+// past the brick's outer radius moving out for good also ends
+// (outbound_for_good, bhn_grrt.cuh): nothing later is sampled.
 
 #include "bhn_exact.cuh"
 #include "bhn_transfer.cuh"
