@@ -420,13 +420,13 @@ def bench_ours(args) -> dict | None:
         accuracy = studies.fine_step_check(db64, view, crop, config=cfg)
         del db64
 
-    # BASELINE's second metric (outside the timed region, rank 0 of a 1-GPU run):
+    # the second half of the metric (outside the timed region, rank 0 of a 1-GPU run):
     # time to a 2048^2 image at <= 1e-3 Stokes-I rel L1, learned step size
     # against the step-doubling controller and the fastest plain step
     tti = None
     if rank == 0 and world == 1 and not args.no_time_to_image:
         tti = time_to_image(device, 2048, 3)
-    # BASELINE config 4 in brief (the full record is `--workload views`): the
+    # the batched-views workload in brief (the full record is `--workload views`): the
     # 256 seeded uneven views in one CUDA-graph launch, aggregate rate
     views_block = None
     if rank == 0 and world == 1 and not args.no_views:
@@ -1398,7 +1398,7 @@ def plain_cpu_time_to_image(brick, view, side: int, target_s: float) -> dict:
 
 
 def bench_learned(args) -> dict | None:
-    """BASELINE's second metric on its own line: time to an image at <= 1e-3
+    """The metric's second half on its own line: time to an image at <= 1e-3
     Stokes-I rel L1, learned step size against plain RK2 and the controller
     (time_to_image)."""
     import torch

@@ -247,7 +247,8 @@ def test_full_image1024_properties(scene_brick):
 @pytest.mark.parametrize("name,spin,incl,side,steps,seed", [("c2", 0.9375, 17.0, 1024, 4096, 0),
                                                               ("c3", 0.998, 60.0, 4096, 8192, 3)])
 def test_fp32_ends_rays_as_fp64_does(name, spin, incl, side, steps, seed):
-    """BASELINE configs 2 and 3 at full size, the reference's semantics
+    """The 1024^2 (a = 0.9375, i = 17 deg) and 4096^2 (a = 0.998, i = 60 deg)
+    workloads at full size, the reference's semantics
     (horizon guard off): no ray ends non-finite in FP32 where the FP64 method
     stays finite (FP32 steps that overflow are taken in FP64), no ray runs to
     max_steps in FP32 alone (midpoints past a pole clip like kerr.py:35-36),
