@@ -1067,7 +1067,7 @@ def bench_bricks(args) -> dict | None:
                      "traffic": profiled_traffic(BRICKS_PROFILE),
                      "traffic_source": f"ncu capture of the same workload ({BRICKS_PROFILE.relative_to(REPO)})",
                      "peak_source": "measured in this run (bhn_fp64_peak_probe FMA chains)",
-                     "kernel": ("brick_trace_pair_kernel" if (pixels + 31) // 32 <= 8 * torch.cuda.get_device_properties(
+                     "kernel": ("brick_trace_pair_kernel" if (pixels + 31) // 32 <= 4 * torch.cuda.get_device_properties(
                          device).multi_processor_count else "brick_trace_kernel"),
                      "algorithmic_flops_per_launch": flops,
                      "flop_per_rk4_step": FP64_FLOP_PER_RK4_STEP, "flop_per_segment": FP64_FLOP_PER_SEGMENT},

@@ -11,7 +11,7 @@
 // nan_to_num(nan = posinf = neginf = 0).  Unlike the fused renderer
 // (bhn_render_launch: the RK2 step h = 0.02 r), this is the reference
 // Python's method: one thread per ray (brick_trace_kernel), or, for images of
-// at most 8 ray warps per SM, two warps per 32 rays (brick_trace_pair_kernel:
+// at most 4 ray warps per SM, two warps per 32 rays (brick_trace_pair_kernel:
 // a geodesic warp and a transfer warp joined by an mbarrier ring).  A ray
 // past the brick's outer radius moving out for good also ends
 // (outbound_for_good, bhn_grrt.cuh): nothing later is sampled.
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(128, 4) brick_trace_kernel(const BrickTracePar
 // optical depth -- and reports the cutoff back.  Same arithmetic, same image.
 constexpr int kRing = 32;
 #ifndef BHN_PAIR_WARPS_PER_SM
-#define BHN_PAIR_WARPS_PER_SM 8
+#define BHN_PAIR_WARPS_PER_SM 4
 #endif
 constexpr int kPairWarpsPerSm = BHN_PAIR_WARPS_PER_SM;  // the two-warp form up to this many ray warps per SM
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s: a wait that long is a fault, not a delay
@@ -348,8 +348,9 @@ extern "C" int bhn_brick_trace_render(const void *coeffs, const double *r_grid, 
     P.max_tau = cfg->max_optical_depth;
     P.out = out;
     P.diag = diag;
-    // Two warps per 32 rays while the one-warp form would leave schedulers idle (at most two warps
-    // per scheduler, 4 per SM); above that the one-warp form's throughput wins.
+    // Two warps per 32 rays while the one-warp form would leave schedulers idle (at most one ray
+    // warp per scheduler, 4 per SM); above that the one-warp form wins (200 x 112, 4.7 ray warps
+    // per SM: 6.52 against 7.17 ms; 256 x 144, 7.8 per SM: even; 160 x 90, 3 per SM: 4.33 against 6.3).
     const int64_t warps = (rays + 31) / 32;
     if (warps <= (int64_t)kPairWarpsPerSm * sm_count_current_device()) {
         unsigned *flags = &reinterpret_cast<QueueState *>(static_cast<unsigned char *>(scratch) +
